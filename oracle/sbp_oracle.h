@@ -1,0 +1,102 @@
+/*
+ * CPU oracle for the SBP-SAT Euler hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A C++17 restatement of the reference's FP64 (and, for the operators, FP32)
+ * arithmetic, operation by operation and in the reference's rounding order.
+ * It is the checker for the CUDA library: only the tests, the smoke entry
+ * point and the CPU-baseline leg of the benchmark load it.  The product never
+ * links or calls it.
+ *
+ * Parity status: the reference (a Rust workspace needing an era-specific
+ * nightly toolchain) cannot be compiled in this environment and ships no
+ * golden vectors, so bit-level agreement with the reference binary is
+ * UNPINNED.  The restatement is pinned instead against every known-answer
+ * test the reference holds for this path: polynomial exactness of all six
+ * operators (sbp/src/operators/{upwind4,upwind9,traditional4,traditional8,
+ * upwind4h2,upwind9h2}.rs tests), the H-norm of ones (euler/src/lib.rs:434-448),
+ * h2linspace (sbp/src/utils.rs:142-155) and the vortex convergence rates
+ * (euler/tests/convergence.rs:54-90).
+ *
+ * Conventions: fields are C-order (4, ny, nx) arrays of (rho, rhou, rhov, e)
+ * (euler/src/lib.rs:215-219); metrics are five (ny, nx) planes in the order
+ * detj, detj*dxi/dx, detj*dxi/dy, detj*deta/dx, detj*deta/dy
+ * (sbp/src/grid.rs:95-140); directions are indexed north, south, east, west.
+ */
+#ifndef SBP_ORACLE_H
+#define SBP_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_UPWIND4 = 0, ORC_UPWIND4H2 = 1, ORC_UPWIND9 = 2, ORC_UPWIND9H2 = 3, ORC_SBP4 = 4, ORC_SBP8 = 5 };
+enum { ORC_DIFF = 0, ORC_DISS = 1 };
+enum { ORC_XI = 0, ORC_ETA = 1 };
+enum { ORC_F64 = 0, ORC_F32 = 1 };
+enum { ORC_BC_THIS = 0, ORC_BC_GRID = 1, ORC_BC_VORTEX = 2 };
+enum { ORC_NORTH = 0, ORC_SOUTH = 1, ORC_EAST = 2, ORC_WEST = 3 };
+
+typedef struct {
+    int nvortices; /* 0..5 */
+    double x0[5], y0[5], rstar[5], eps[5];
+    double mach;
+} orc_vortex_params;
+
+typedef struct {
+    int64_t nx, ny;
+    int op_xi, op_eta;
+    const double* x; /* (ny, nx) */
+    const double* y; /* (ny, nx) */
+    int bc_kind[4];  /* ORC_BC_* per direction N, S, E, W */
+    int bc_neighbour[4];
+} orc_block_desc;
+
+typedef struct orc_system orc_system;
+
+/* Operator tables.  part: 0 start block (M*N), 1 diagonal (D), 2 end block (M*N), 3 H weights (M).
+ * Returns the number of values written, or -1. */
+int orc_op_table(int op, int kind, int part, int dtype, void* out);
+int orc_op_shape(int op, int* m, int* n, int* d, int* is_h2, int* is_upwind);
+
+/* SbpOperator2d::diffxi/diffeta and UpwindOperator2d::dissxi/disseta on a C-order (ny, nx) array. */
+int orc_op_apply(int op, int dir, int kind, int dtype, const void* in, void* out, int64_t ny, int64_t nx);
+
+/* Grid::metrics (sbp/src/grid.rs:95-140); out = 5*(ny*nx).  Returns -2 if detj <= 0. */
+int orc_metrics(int op_xi, int op_eta, const double* x, const double* y, int64_t ny, int64_t nx, double* out);
+
+/* VortexParameters::evaluate (euler/src/vortex.rs:26-113) at n points; q gets 4 planes of n. */
+int orc_vortex(const orc_vortex_params* vp, double gamma, double t, const double* x, const double* y,
+               int64_t n, double* q);
+
+/* RHS_upwind (or RHS_trad when not both operators are upwind) with SAT_characteristics, given
+ * boundary data z[d] (4 x edge length, component-major) for d = N, S, E, W. */
+int orc_rhs(int op_xi, int op_eta, double gamma, const double* q, const double* metrics,
+            const double* zn, const double* zs, const double* ze, const double* zw,
+            int64_t ny, int64_t nx, int force_trad, double* k);
+
+/* Field::h2_err (euler/src/lib.rs:377-431) */
+double orc_h2_err(int op_xi, int op_eta, const double* a, const double* b, int64_t ny, int64_t nx);
+
+/* Multi-block system with the single-threaded multigrid semantics
+ * (multigrid/src/system.rs:456-636). */
+orc_system* orc_system_create(const orc_block_desc* blocks, int nblocks, double gamma);
+void orc_system_destroy(orc_system* s);
+int orc_system_set_vortex(orc_system* s, const orc_vortex_params* vp);
+int orc_system_init_vortex(orc_system* s, double t);
+int orc_system_set_state(orc_system* s, int block, const double* q);
+int orc_system_get_state(const orc_system* s, int block, double* q);
+int orc_system_get_metrics(const orc_system* s, int block, double* out);
+/* nsteps of RK4 with the given dt; force_trad selects RHS_trad (euler::System::advance). */
+int orc_system_advance(orc_system* s, int64_t nsteps, double dt, int force_trad);
+double orc_system_time(const orc_system* s);
+void orc_system_set_time(orc_system* s, double t);
+double orc_system_max_dt(const orc_system* s);
+double orc_system_error(const orc_system* s);
+/* Advance independent systems concurrently on nthreads host threads, each its own steps and dt. */
+int orc_systems_advance(orc_system** systems, int n, const int64_t* nsteps, const double* dt, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
