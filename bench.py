@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark: Euler RK4 point-updates/s on one B200, batched FP32 (compensated) vs plain FP64.
+
+Workload (one "step" = one RK4 step of every instance): the batched ensemble -- 512
+independent isentropic-vortex solves drawn from SplitMix64 seed 1 (centre ~ U[-2,2]^2,
+eps ~ U[0.5,1.5], Mach ~ U[0.3,0.7], side ~ U{48..257}, Upwind4/Upwind9 50/50) on single
+warped curvilinear blocks with vortex SATs on every edge, each with its own dt = 0.2/(side-1).
+Synthetic inputs: the reference has no dataset.  Under torchrun each rank runs its own 512
+instances (the next 512 of the same stream): weak scaling, no data-path collective.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Euler RK4 point-updates/s, 1 B200: batched FP32 vs plain FP64 at same L2 error"
+UNIT = "point-updates/s"
+# Algorithmic HBM bytes per point-update of the fused stage design (sum over the 4 stage
+# launches of the state, accumulator and metric planes each launch must read and write once).
+BYTES_PER_POINT_UPDATE = {"f32c": 464, "f64": 672}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--ninst", type=int, default=512)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(
+        os.environ.get("WORLD_SIZE", "1"))
+
+
+# ------------------------------------------------------------------------------------------
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def recorded_traffic(precision: str):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary, scaled per point."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(precision)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------------------------------
+def build_system(insts, precision, device):
+    from summationbyparts_b200 import workloads
+    from summationbyparts_b200.system import BlockSystem
+    blocks = workloads.ensemble_blocks(insts)
+    s = BlockSystem(blocks, len(insts), precision, 1.4, device)
+    for k, inst in enumerate(insts):
+        s.set_vortex(inst.vortex, k)
+        s.set_dt(inst.dt, k)
+    s.init_vortex(0.0)
+    return s
+
+
+def timed_advance(torch, s, stream, steps, barrier):
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def cpu_baseline(insts, seconds, nthreads, steps_per_sample=1):
+    """The oracle (C++ port of the reference arithmetic) on the host cores: time one step of a
+    bounded sample of instances, all threads.  Returns (point-updates/s, description)."""
+    from oracle import oracle as orc
+    from summationbyparts_b200 import workloads
+    # calibrate on one small instance
+    small = min(insts, key=lambda i: i.side)
+    blk = workloads.ensemble_blocks([small])[0]
+    s = orc.System([dict(x=blk.x, y=blk.y, op_xi=small.op_id, op_eta=small.op_id, bc=list(blk.bc))], fast=True)
+    s.set_vortex([dict(x0=small.x0, y0=small.y0, rstar=0.5, eps=small.eps)], small.mach)
+    s.init_vortex(0.0)
+    t0 = time.perf_counter()
+    s.advance(1, small.dt)
+    per_point = (time.perf_counter() - t0) / (small.side ** 2)
+    budget_points = seconds * nthreads / max(per_point, 1e-9) / steps_per_sample
+    # round-robin sample so the operator and size mix follows the ensemble
+    order = insts[::max(1, len(insts) // 64)] + insts
+    sample, pts = [], 0
+    for inst in order:
+        if inst in sample:
+            continue
+        if pts + inst.side ** 2 > budget_points and sample:
+            break
+        sample.append(inst)
+        pts += inst.side ** 2
+    systems = []
+    for inst in sample:
+        b = workloads.ensemble_blocks([inst])[0]
+        so = orc.System([dict(x=b.x, y=b.y, op_xi=inst.op_id, op_eta=inst.op_id, bc=list(b.bc))], fast=True)
+        so.set_vortex([dict(x0=inst.x0, y0=inst.y0, rstar=0.5, eps=inst.eps)], inst.mach)
+        so.init_vortex(0.0)
+        systems.append(so)
+    t0 = time.perf_counter()
+    orc.advance_many(systems, [steps_per_sample] * len(systems), [i.dt for i in sample], nthreads)
+    dt = time.perf_counter() - t0
+    return pts * steps_per_sample / dt, {"instances": len(sample), "points": pts, "steps": steps_per_sample,
+                                         "seconds": dt}
+
+
+# ------------------------------------------------------------------------------------------
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    from summationbyparts_b200 import workloads
+    insts = workloads.ensemble_instances(args.ninst, seed=1)
+    nthreads = os.cpu_count() or 1
+    per_step = max(1.0, min(4.0, 120.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(insts, per_step * 0.25, nthreads)
+    vals, descs = [], []
+    for _ in range(args.steps):
+        v, d = cpu_baseline(insts, per_step, nthreads)
+        vals.append(v)
+        descs.append(d)
+    value = statistics.mean(vals)
+    ms = 1e3 * statistics.mean(d["seconds"] for d in descs)
+    sample = (f"{descs[0]['instances']} of {len(insts)} instances ({descs[0]['points']} points), "
+              f"1 RK4 step per timed step, {nthreads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched ensemble, 512 vortex solves (SplitMix64 seed 1), sides 48-257, "
+                                   "Upwind4/Upwind9, vortex SATs", "instances": args.ninst},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+        def barrier():
+            dist.barrier()
+    else:
+        def barrier():
+            pass
+
+    from summationbyparts_b200 import workloads
+    insts = workloads.ensemble_instances(args.ninst, seed=1, first=rank * args.ninst)
+    points = workloads.ensemble_points(insts)
+    stream = torch.cuda.Stream()
+    s32 = build_system(insts, "f32c", local)
+    s32.set_stream(stream.cuda_stream)
+    tiles = s32.autotune()
+    for _ in range(args.warmup):
+        s32.advance(1)
+    clocks = Clocks(local)
+    clocks.start()
+    ms = timed_advance(torch, s32, stream, args.steps, barrier)
+    clk = clocks.stop()
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    total_points = points * world
+    value = total_points * args.steps / (ms / 1e3)
+    ms_step = ms / args.steps
+    launches = s32.launches_per_step() * args.steps
+
+    # FP64 plain form on the same ensemble
+    fp64 = None
+    acc = None
+    if not args.no_fp64:
+        s64 = build_system(insts, "f64", local)
+        s64.set_stream(stream.cuda_stream)
+        t64 = s64.autotune()
+        for _ in range(args.warmup):
+            s64.advance(1)
+        ms64 = timed_advance(torch, s64, stream, args.steps, barrier)
+        t = torch.tensor([ms64], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms64 = float(t.item())
+        v64 = total_points * args.steps / (ms64 / 1e3)
+        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "tiles": list(t64),
+                "speedup_f32_over_f64": value / v64}
+        # same-error check: both forms advanced warmup+steps steps from the same initial data
+        e32, e64 = s32.errors(), s64.errors()
+        import numpy as np
+        rel = np.abs(e32 - e64) / e64
+        n = s32.state_count(0)
+        a = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        b = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        s32.get_state_all(a)
+        s64.get_state_all(b)
+        d = (a - b).norm().item() / b.norm().item()
+        acc = {"steps": args.warmup + args.steps, "l2_err_f64_median": float(np.median(e64)),
+               "l2_err_f32c_median": float(np.median(e32)), "err_rel_diff_max": float(rel.max()),
+               "state_rel_l2_f32c_vs_f64": d}
+        s64.close()
+
+    # end to end through the C ABI with host buffers: per step, upload the state from pinned host
+    # memory, advance one RK4 step, read the new state back (euler::System::advance_upwind + field())
+    e2e = None
+    if not args.no_e2e:
+        n = s32.state_count(0)
+        host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        s32.get_state_all(host)
+        ke = max(3, min(args.steps, 10))
+        for _ in range(2):
+            s32.set_state_all(host)
+            s32.advance(1)
+            s32.get_state_all(host)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            s32.set_state_all(host)
+            s32.advance(1)
+            s32.get_state_all(host)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        me = e0.elapsed_time(e1)
+        t = torch.tensor([me], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        me = float(t.item())
+        e2e = {"value": total_points * ke / (me / 1e3), "unit": UNIT, "h2d_bytes_per_step": n * 8,
+               "d2h_bytes_per_step": n * 8, "steps": ke,
+               "path": "sbp_system_set_state_all + sbp_system_advance(1) + sbp_system_get_state_all, f64 host state"}
+
+    peak, peak_kind = measured_hbm_peak()
+    bpp = BYTES_PER_POINT_UPDATE["f32c"]
+    launches_stage = 4 * (s32.launches_per_step() - 1) // 4
+    bytes_per_launch = bpp * points / 4.0  # average over the 4 stage launches of a step
+    achieved = bpp * points / (ms_step / 1e3) / 1e9
+    traffic = recorded_traffic("f32c")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": (traffic * points / 4.0) if traffic else None,
+            "kernel": "stage_kernel (fused RK4 stage)", "algorithmic_bytes_per_point_update": bpp,
+            "bytes_per_launch": bytes_per_launch, "stage_launches_per_step": launches_stage,
+            "peak_source": f"{peak_kind} hbm_gbs"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        v, d = cpu_baseline(insts, args.cpu_seconds, nthreads)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"{d['instances']} of {len(insts)} instances ({d['points']} points), 1 RK4 step, "
+                         f"{nthreads} threads, {d['seconds']:.1f} s"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched ensemble: 512 vortex solves per GPU (SplitMix64 seed 1), sides 48-257, "
+                                       "Upwind4/Upwind9 50/50, warped single blocks, vortex SATs, FP32 compensated RK4",
+                           "instances_per_gpu": len(insts), "points_per_gpu": points, "precision": "f32c",
+                           "tiles": list(tiles), "l2": f"inputs larger than L2 (state+metrics "
+                                                       f"{points * 4 * (8 + 8 + 4 + 4 + 5) / 1e6:.0f} MB per GPU)",
+                           "parallelism": f"ensemble sharded, {world} rank(s), no collective"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "fp64_plain": fp64, "accuracy": acc}
+        print(json.dumps(line), flush=True)
+    s32.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

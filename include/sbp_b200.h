@@ -1,0 +1,198 @@
+/*
+ * sbp_b200 -- B200-native (sm_100a) SBP-SAT Euler time stepping, C ABI.
+ *
+ * This is the drop-in boundary for the reference's hot path (mulimoen/
+ * SummationByParts): the SbpOperator2d / UpwindOperator2d stencils, the Euler
+ * right-hand side with its SATs, and the RK4 stage update, plus the
+ * euler::System / multigrid::System driver surface that calls them.  The
+ * reference has no FFI of its own; each entry point below names the Rust item
+ * it replaces.  A Rust -sys crate binds exactly these symbols (see
+ * INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every function returns sbp_status (0 = SBP_OK) unless noted; on error a
+ *    message is available from sbp_last_error() (thread-local).  Nothing in
+ *    the library aborts or exits.
+ *  - Fields are C-order (4, ny, nx) arrays of (rho, rhou, rhov, e), the
+ *    reference's euler::Field layout (euler/src/lib.rs:190-219).  2-D arrays
+ *    are (ny, nx) with x (xi) contiguous.
+ *  - Pointers named d_* are device pointers; others are host pointers.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *  - Directions are indexed SBP_NORTH, SBP_SOUTH, SBP_EAST, SBP_WEST.
+ */
+#ifndef SBP_B200_H
+#define SBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sbp_status {
+    SBP_OK = 0,
+    SBP_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad enum, bad index */
+    SBP_ERR_SHAPE = 2,            /* n < max(2M, N), mismatched interface lengths, ... */
+    SBP_ERR_UNSUPPORTED = 3,      /* combination not built (e.g. dissipation of SBP4) */
+    SBP_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    SBP_ERR_NONPHYSICAL = 5,      /* rho <= 0, p <= 0, detJ <= 0 or NaN detected on device */
+    SBP_ERR_NO_DEVICE = 6,
+    SBP_ERR_OUT_OF_MEMORY = 7
+} sbp_status;
+
+/* The six operators of sbp/src/operators.rs:152-165. */
+typedef enum sbp_operator {
+    SBP_OP_UPWIND4 = 0,
+    SBP_OP_UPWIND4H2 = 1,
+    SBP_OP_UPWIND9 = 2,
+    SBP_OP_UPWIND9H2 = 3,
+    SBP_OP_SBP4 = 4,
+    SBP_OP_SBP8 = 5
+} sbp_operator;
+
+typedef enum sbp_dtype { SBP_F64 = 0, SBP_F32 = 1 } sbp_dtype;
+
+/* SBP_PRECISION_F64: the reference's f64 arithmetic, operation for operation.
+ * SBP_PRECISION_F32_COMPENSATED: stencils, fluxes and dissipation in f32, the RK4 state kept as
+ * a compensated (hi, lo) f32 pair; metrics built in f64, SAT terms and norms in f64. */
+typedef enum sbp_precision { SBP_PRECISION_F64 = 0, SBP_PRECISION_F32_COMPENSATED = 1 } sbp_precision;
+
+/* euler::BoundaryCharacteristic (euler/src/lib.rs:737-745): This, Grid(neighbour), Vortex. */
+typedef enum sbp_boundary_kind { SBP_BC_THIS = 0, SBP_BC_GRID = 1, SBP_BC_VORTEX = 2 } sbp_boundary_kind;
+
+enum { SBP_NORTH = 0, SBP_SOUTH = 1, SBP_EAST = 2, SBP_WEST = 3 };
+
+/* euler::VortexParameters (euler/src/vortex.rs:4-21): up to 5 superposed vortices. */
+typedef struct sbp_vortex_params {
+    int nvortices;
+    double x0[5], y0[5], rstar[5], eps[5];
+    double mach;
+} sbp_vortex_params;
+
+/* One curvilinear block: its grid (sbp::grid::Grid, sbp/src/grid.rs:9-35), its operator pair
+ * (the (eta, xi) tuple of sbp/src/operators.rs:115-150), its four boundary kinds and the
+ * independent solve ("instance") it belongs to.  Blocks of one instance share dt, time and
+ * vortex parameters; instances are independent (an ensemble). */
+typedef struct sbp_block_desc {
+    int64_t nx, ny;
+    int op_xi, op_eta;    /* sbp_operator */
+    const double* x;      /* host, (ny, nx) */
+    const double* y;      /* host, (ny, nx) */
+    int bc_kind[4];       /* sbp_boundary_kind per direction */
+    int bc_neighbour[4];  /* block index for SBP_BC_GRID */
+    int instance;         /* 0 .. ninstances-1 */
+} sbp_block_desc;
+
+typedef struct sbp_system sbp_system;
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* sbp_last_error(void);
+/* Library version string. */
+const char* sbp_version(void);
+
+/* ---- operators: SbpOperator1d / SbpOperator2d / UpwindOperator2d -------- */
+
+/* SbpOperator1d::h (sbp/src/operators.rs:15-16): writes the M boundary weights of H into h
+ * (capacity cap) and returns M, or -1 for a bad operator. */
+int sbp_operator_h(int op, double* h, int cap);
+/* SbpOperator1d::is_h2 (sbp/src/operators.rs:17-20): 1, 0, or -1 for a bad operator. */
+int sbp_operator_is_h2(int op);
+/* SbpOperator2d::upwind().is_some() (sbp/src/operators.rs:85-87): 1, 0, or -1. */
+int sbp_operator_is_upwind(int op);
+/* Coefficients as built into the kernels, for verification against the reference tables:
+ * kind 0 = first derivative (DIFF), 1 = dissipation (DISS); part 0 = start block (M*N),
+ * 1 = interior diagonal (D), 2 = end block (M*N).  Returns the count written, or -1. */
+int sbp_operator_table(int op, int kind, int part, double* out, int cap);
+
+/* SbpOperator2d::diffxi (sbp/src/operators.rs:56-61; algos.rs:101-187 row path):
+ * for each of nbatch (ny, nx) arrays spaced batch_stride elements apart, differentiate along x.
+ * Results are bit-identical to the reference's row path in the same dtype. */
+sbp_status sbp_diffxi(int op, int dtype, const void* d_prev, void* d_fut, int64_t ny, int64_t nx,
+                      int64_t nbatch, int64_t batch_stride, void* stream);
+/* SbpOperator2d::diffeta (sbp/src/operators.rs:62-64; algos.rs:371-519 column path). */
+sbp_status sbp_diffeta(int op, int dtype, const void* d_prev, void* d_fut, int64_t ny, int64_t nx,
+                       int64_t nbatch, int64_t batch_stride, void* stream);
+/* UpwindOperator2d::dissxi (sbp/src/operators.rs:91-96). */
+sbp_status sbp_dissxi(int op, int dtype, const void* d_prev, void* d_fut, int64_t ny, int64_t nx,
+                      int64_t nbatch, int64_t batch_stride, void* stream);
+/* UpwindOperator2d::disseta (sbp/src/operators.rs:98-100). */
+sbp_status sbp_disseta(int op, int dtype, const void* d_prev, void* d_fut, int64_t ny, int64_t nx,
+                       int64_t nbatch, int64_t batch_stride, void* stream);
+
+/* Grid::metrics / Metrics::new (sbp/src/grid.rs:64-140) in f64 on device:
+ * d_metrics receives 5 planes (detj, detj*dxi/dx, detj*dxi/dy, detj*deta/dx, detj*deta/dy).
+ * Returns SBP_ERR_NONPHYSICAL if detj <= 0 anywhere (the reference asserts). */
+sbp_status sbp_metrics(int op_xi, int op_eta, const double* d_x, const double* d_y, int64_t ny, int64_t nx,
+                       double* d_metrics, void* stream);
+
+/* ---- systems: euler::System, multigrid::System, ensembles --------------- */
+
+/* Build a system on `device`: copies the grids in, builds the f64 metrics on the device
+ * (BaseSystem::create, multigrid/src/system.rs:55-78) and allocates state and stage buffers.
+ * State starts at zero; instance dt starts at NaN and time at 0 (system.rs:126-128). */
+sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nblocks, int ninstances,
+                             int precision, double gamma, sbp_system** out);
+sbp_status sbp_system_destroy(sbp_system* sys);
+
+/* Use RHS_trad even for upwind operators (euler::System::advance, euler/src/lib.rs:50-81)
+ * when force_trad != 0; otherwise RHS_upwind when both operators are upwind (system.rs:520-526). */
+sbp_status sbp_system_set_force_trad(sbp_system* sys, int force_trad);
+
+/* Vortex parameters of one instance (or all when instance < 0); used by vortex initial data,
+ * SBP_BC_VORTEX boundaries and sbp_system_error. */
+sbp_status sbp_system_set_vortex(sbp_system* sys, int instance, const sbp_vortex_params* vp);
+/* Field::vortex / SingleThreadedSystem::vortex (euler/src/lib.rs:319-328, system.rs:477-481):
+ * state of every block of the instance(s) := the vortex at time t.  instance < 0 = all. */
+sbp_status sbp_system_init_vortex(sbp_system* sys, int instance, double t);
+
+/* Host <-> device state of one block, (4, ny, nx) f64 (the f32 state is widened / rounded). */
+sbp_status sbp_system_set_state(sbp_system* sys, int block, const double* q);
+sbp_status sbp_system_get_state(sbp_system* sys, int block, double* q);
+/* All blocks at once, concatenated in block order; for a compensated system the state is
+ * 2 x (4, ny, nx) f32 per block (hi then lo) when dtype = SBP_F32, else widened f64. */
+sbp_status sbp_system_set_state_all(sbp_system* sys, int dtype, const void* q);
+sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q);
+/* Number of state elements of sbp_system_{set,get}_state_all for dtype. */
+int64_t sbp_system_state_count(const sbp_system* sys, int dtype);
+
+/* dt / time of one instance (instance < 0 = all).  System::set_dt (system.rs:396-405). */
+sbp_status sbp_system_set_dt(sbp_system* sys, int instance, double dt);
+sbp_status sbp_system_set_time(sbp_system* sys, int instance, double t);
+sbp_status sbp_system_get_time(sbp_system* sys, int instance, double* t);
+
+/* SingleThreadedSystem::max_dt (multigrid/src/system.rs:542-589) over the blocks of one instance. */
+sbp_status sbp_system_max_dt(sbp_system* sys, int instance, double* dt);
+
+/* SingleThreadedSystem::advance (system.rs:491-498): nsteps RK4 steps of every instance, each
+ * with its own dt; four fused stage launches per step, replayed as one CUDA graph. */
+sbp_status sbp_system_advance(sbp_system* sys, int64_t nsteps);
+/* Ragged ensemble advance: instance i takes nsteps[i] steps; finished instances drop out of the
+ * launch schedule.  Blocks until done. */
+sbp_status sbp_system_advance_instances(sbp_system* sys, const int64_t* nsteps);
+
+/* SingleThreadedSystem::error (system.rs:618-635): sum over the instance's blocks of
+ * Field::h2_err against the vortex at the instance time.  per_instance has ninstances entries. */
+sbp_status sbp_system_error(sbp_system* sys, double* per_instance);
+/* Field::h2_err (euler/src/lib.rs:377-431) of one block's state against a host field q. */
+sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double* err);
+
+/* Tile schedule: output tiles of ty x tx points per CTA, `threads` threads per CTA
+ * (0 = keep).  sbp_system_autotune times the candidate schedules on the current state
+ * (state and time are restored) and keeps the fastest. */
+sbp_status sbp_system_set_tiles(sbp_system* sys, int ty, int tx, int threads);
+sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads);
+
+/* Stream the system launches on (cudaStream_t as void*; NULL = a stream owned by the system). */
+sbp_status sbp_system_set_stream(sbp_system* sys, void* stream);
+/* Device pointer to one block's current state plane set (f64 or f32 hi), for zero-copy use. */
+sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q);
+/* Kernel launches per RK4 step (the stage kernels plus the time update). */
+int sbp_system_launches_per_step(const sbp_system* sys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBP_B200_H */

@@ -1,0 +1,15 @@
+// Lookup of the instantiated fused stage kernels (stage_*.cu).
+#pragma once
+
+namespace sbp {
+// prec 0 = f64, 1 = f32 compensated.  Returns the kernel entry (a __global__ function pointer
+// usable with cudaLaunchKernel) or nullptr if that operator pair was not built.
+const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw);
+
+const void* stage_ptr_f64_u4(int opx, int opy, bool upw);
+const void* stage_ptr_f64_u9(int opx, int opy, bool upw);
+const void* stage_ptr_f64_sbp(int opx, int opy, bool upw);
+const void* stage_ptr_f32_u4(int opx, int opy, bool upw);
+const void* stage_ptr_f32_u9(int opx, int opy, bool upw);
+const void* stage_ptr_f32_sbp(int opx, int opy, bool upw);
+}  // namespace sbp

@@ -1,0 +1,1020 @@
+// Systems of curvilinear blocks on one GPU: the euler::System / multigrid::System surface and
+// ensembles of independent solves (instances), behind the C ABI.
+//
+// Per RK4 step the device runs, for each of the 4 stages, one persistent fused stage kernel per
+// operator pair present (all tiles of all active blocks of that pair in one launch), then one
+// tiny kernel that advances the instance times.  The whole step is captured once as a CUDA
+// graph and replayed; the graph is re-captured only when the tile schedule or the set of
+// active instances changes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "euler_device.cuh"
+#include "op_apply.h"
+#include "sbp_ops.cuh"
+#include "stage_dispatch.h"
+#include "stage_kernel.cuh"
+#include "system_kernels.h"
+
+namespace sbp {
+const double* op_h_weights(int op);
+
+const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw) {
+    using F = const void* (*)(int, int, bool);
+    static const F f64[] = {stage_ptr_f64_u4, stage_ptr_f64_u9, stage_ptr_f64_sbp};
+    static const F f32[] = {stage_ptr_f32_u4, stage_ptr_f32_u9, stage_ptr_f32_sbp};
+    for (F f : (prec == 0 ? f64 : f32)) {
+        const void* p = f(opx, opy, upw);
+        if (p) return p;
+    }
+    return nullptr;
+}
+
+namespace {
+
+void region_host(int op, int a0, int a1, int n, int& lo, int& hi) {
+    switch (op) {
+        case UPWIND4: region_of<UPWIND4>(a0, a1, n, lo, hi); break;
+        case UPWIND4H2: region_of<UPWIND4H2>(a0, a1, n, lo, hi); break;
+        case UPWIND9: region_of<UPWIND9>(a0, a1, n, lo, hi); break;
+        case UPWIND9H2: region_of<UPWIND9H2>(a0, a1, n, lo, hi); break;
+        case SBP4: region_of<SBP4>(a0, a1, n, lo, hi); break;
+        default: region_of<SBP8>(a0, a1, n, lo, hi); break;
+    }
+}
+
+int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
+
+struct Group {
+    int opx, opy;
+    bool upw;
+    const void* fn;
+    int4* d_tiles = nullptr;
+    int ntiles = 0;
+    int WX = 0, HY = 0;
+    size_t smem = 0;
+    int grid = 0;
+};
+
+}  // namespace
+}  // namespace sbp
+
+using namespace sbp;
+
+struct sbp_system {
+    int device = 0;
+    int prec = 0;
+    double gamma = 1.4;
+    bool force_trad = false;
+    int nblocks = 0, ninst = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    std::vector<BlockDev> hb;
+    std::vector<InstanceDev> hi;
+    int64_t nq = 0, nm = 0, nx2 = 0, max_points = 0, dense_total = 0;
+    std::vector<int64_t> dense_off;  // packed (4, ny, nx) offsets
+    // device memory
+    BlockDev* d_blocks = nullptr;
+    InstanceDev* d_inst = nullptr;
+    int* d_active = nullptr;
+    void *prev_hi = nullptr, *prev_lo = nullptr, *acc_hi = nullptr, *acc_lo = nullptr, *uA = nullptr, *uB = nullptr;
+    double* met64 = nullptr;
+    float* met32 = nullptr;
+    double* xy = nullptr;
+    double* hw = nullptr;
+    int64_t* d_hoff = nullptr;
+    std::vector<int64_t> hoff;
+    int64_t* d_poff4 = nullptr;  // packed offsets in elements for dtype f64 (4n per block)
+    int64_t* d_poff8 = nullptr;  // packed offsets for dtype f32 hi+lo (8n per block)
+    int64_t* d_zero = nullptr;
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    unsigned* status = nullptr;
+    double* d_sums = nullptr;
+    unsigned long long* d_speeds = nullptr;
+    // schedule
+    int TY = 32, TX = 32, threads = 256;
+    std::vector<int> active;
+    std::vector<Group> groups;
+    bool sched_dirty = true;
+    cudaStream_t stream = nullptr;
+    cudaStream_t user_stream = nullptr;
+    bool has_user_stream = false;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t ev_fork = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+
+    cudaStream_t st() const { return has_user_stream ? user_stream : stream; }
+    size_t tsize() const { return prec == 0 ? sizeof(double) : sizeof(float); }
+};
+
+namespace {
+
+void free_groups(sbp_system* s) {
+    for (auto& g : s->groups) cudaFree(g.d_tiles);
+    s->groups.clear();
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->gexec = nullptr;
+    s->graph = nullptr;
+}
+
+void destroy_all(sbp_system* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_groups(s);
+    void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
+                    s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
+                    s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto st : s->side) cudaStreamDestroy(st);
+    for (auto e : s->ev) cudaEventDestroy(e);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+sbp_status upload_instances(sbp_system* s) {
+    SBP_TRY_CUDA(cudaMemcpyAsync(s->d_inst, s->hi.data(), s->hi.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice,
+                                 s->st()));
+    return SBP_OK;
+}
+
+// Pull device-advanced instance times into the host copy before editing it.
+sbp_status sync_times(sbp_system* s) {
+    std::vector<InstanceDev> tmp(s->hi.size());
+    SBP_TRY_CUDA(cudaMemcpyAsync(tmp.data(), s->d_inst, tmp.size() * sizeof(InstanceDev), cudaMemcpyDeviceToHost,
+                                 s->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(s->st()));
+    for (size_t i = 0; i < tmp.size(); ++i) s->hi[i].time = tmp[i].time;
+    return SBP_OK;
+}
+
+void set_dt_host(InstanceDev& I, double dt) {
+    // Tableau entries times dt exactly as integrate() forms them (utils/integrate/src/lib.rs:30-35,
+    // 193-211): a*dt for the stage states and b*dt for the final combination.
+    I.dt = dt;
+    I.ca[0] = 0.5 * dt;
+    I.ca[1] = 0.5 * dt;
+    I.ca[2] = 1.0 * dt;
+    I.cb[0] = (1.0 / 6.0) * dt;
+    I.cb[1] = (1.0 / 3.0) * dt;
+    I.cb[2] = (1.0 / 3.0) * dt;
+    I.cb[3] = (1.0 / 6.0) * dt;
+}
+
+template <class T>
+StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
+    StageArgs<T> a{};
+    a.blocks = s->d_blocks;
+    a.inst = s->d_inst;
+    a.tiles = g.d_tiles;
+    a.ntiles = g.ntiles;
+    a.stage = stage;
+    a.TY = s->TY;
+    a.TX = s->TX;
+    a.WX = g.WX;
+    a.HY = g.HY;
+    T* prev = static_cast<T*>(s->prev_hi);
+    T* uA = static_cast<T*>(s->uA);
+    T* uB = static_cast<T*>(s->uB);
+    const T* ins[4] = {prev, uA, uB, uA};
+    T* outs[4] = {uA, uB, uA, nullptr};
+    a.u_in = ins[stage];
+    a.u_out = outs[stage];
+    a.prev_hi = prev;
+    a.prev_lo = static_cast<const T*>(s->prev_lo);
+    a.acc_hi = static_cast<T*>(s->acc_hi);
+    a.acc_lo = static_cast<T*>(s->acc_lo);
+    a.new_hi = prev;
+    a.new_lo = static_cast<T*>(s->prev_lo);
+    a.met = s->prec == 0 ? reinterpret_cast<const T*>(s->met64) : reinterpret_cast<const T*>(s->met32);
+    a.met64 = s->met64;
+    a.xy = s->xy;
+    a.gamma = s->gamma;
+    a.status = s->status;
+    return a;
+}
+
+sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st) {
+    if (g.ntiles == 0) return SBP_OK;
+    cudaError_t e;
+    if (s->prec == 0) {
+        StageArgs<double> a = stage_args<double>(s, stage, g);
+        void* args[] = {&a};
+        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+    } else {
+        StageArgs<float> a = stage_args<float>(s, stage, g);
+        void* args[] = {&a};
+        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+    }
+    return cuda_status(e, "stage kernel launch");
+}
+
+// Build per-operator-pair tile lists for the active blocks, size shared memory and grids.
+sbp_status build_schedule(sbp_system* s) {
+    free_groups(s);
+    const int TY = s->TY, TX = s->TX;
+    for (int b = 0; b < s->nblocks; ++b) {
+        const BlockDev& B = s->hb[b];
+        if (!s->active[B.instance]) continue;
+        OpInfo ox, oy;
+        op_info(B.op_xi, ox);
+        op_info(B.op_eta, oy);
+        const bool upw = ox.upwind && oy.upwind && !s->force_trad;
+        Group* gp = nullptr;
+        for (auto& g : s->groups)
+            if (g.opx == B.op_xi && g.opy == B.op_eta && g.upw == upw) gp = &g;
+        if (!gp) {
+            Group g;
+            g.opx = B.op_xi;
+            g.opy = B.op_eta;
+            g.upw = upw;
+            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw);
+            if (!g.fn) {
+                set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", B.op_xi, B.op_eta);
+                return SBP_ERR_UNSUPPORTED;
+            }
+            s->groups.push_back(g);
+            gp = &s->groups.back();
+        }
+    }
+    std::vector<std::vector<int4>> tiles(s->groups.size());
+    for (int b = 0; b < s->nblocks; ++b) {
+        const BlockDev& B = s->hb[b];
+        if (!s->active[B.instance]) continue;
+        OpInfo ox, oy;
+        op_info(B.op_xi, ox);
+        op_info(B.op_eta, oy);
+        const bool upw = ox.upwind && oy.upwind && !s->force_trad;
+        size_t gi = 0;
+        for (; gi < s->groups.size(); ++gi)
+            if (s->groups[gi].opx == B.op_xi && s->groups[gi].opy == B.op_eta && s->groups[gi].upw == upw) break;
+        Group& g = s->groups[gi];
+        for (int y0 = 0; y0 < B.ny; y0 += TY)
+            for (int x0 = 0; x0 < B.nx; x0 += TX) {
+                int lo, hi;
+                region_host(B.op_xi, x0, std::min(x0 + TX, B.nx), B.nx, lo, hi);
+                g.WX = std::max(g.WX, hi - lo);
+                region_host(B.op_eta, y0, std::min(y0 + TY, B.ny), B.ny, lo, hi);
+                g.HY = std::max(g.HY, hi - lo);
+                tiles[gi].push_back(make_int4(b, y0, x0, 0));
+            }
+    }
+    for (size_t gi = 0; gi < s->groups.size(); ++gi) {
+        Group& g = s->groups[gi];
+        g.ntiles = (int)tiles[gi].size();
+        g.smem = s->prec == 0 ? stage_smem_bytes<double>(g.upw, TY, TX, g.WX, g.HY)
+                              : stage_smem_bytes<float>(g.upw, TY, TX, g.WX, g.HY);
+        if (g.smem > s->smem_optin) {
+            set_error("tile %dx%d needs %zu bytes of shared memory (limit %zu)", TY, TX, g.smem, s->smem_optin);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        SBP_TRY_CUDA(cudaFuncSetAttribute(g.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+        int per_sm = 0;
+        SBP_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g.fn, s->threads, g.smem));
+        if (per_sm < 1) {
+            set_error("stage kernel cannot be resident with %d threads and %zu bytes shared memory", s->threads,
+                      g.smem);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        g.grid = std::min(g.ntiles, per_sm * s->num_sms);
+        if (g.ntiles) {
+            SBP_TRY_CUDA(cudaMalloc(&g.d_tiles, g.ntiles * sizeof(int4)));
+            SBP_TRY_CUDA(cudaMemcpyAsync(g.d_tiles, tiles[gi].data(), g.ntiles * sizeof(int4),
+                                         cudaMemcpyHostToDevice, s->stream));
+        }
+    }
+    std::vector<int> act(s->active);
+    SBP_TRY_CUDA(cudaMemcpyAsync(s->d_active, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+    while (s->side.size() < s->groups.size()) {
+        cudaStream_t st;
+        cudaEvent_t e;
+        SBP_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        SBP_TRY_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s->side.push_back(st);
+        s->ev.push_back(e);
+    }
+    // Capture one RK4 step.
+    SBP_TRY_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    sbp_status rc = SBP_OK;
+    for (int stage = 0; stage < 4 && rc == SBP_OK; ++stage) {
+        if (s->groups.size() == 1) {
+            rc = launch_group(s, stage, s->groups[0], s->stream);
+        } else {
+            cudaEventRecord(s->ev_fork, s->stream);
+            for (size_t gi = 0; gi < s->groups.size() && rc == SBP_OK; ++gi) {
+                cudaStreamWaitEvent(s->side[gi], s->ev_fork, 0);
+                rc = launch_group(s, stage, s->groups[gi], s->side[gi]);
+                cudaEventRecord(s->ev[gi], s->side[gi]);
+            }
+            for (size_t gi = 0; gi < s->groups.size(); ++gi) cudaStreamWaitEvent(s->stream, s->ev[gi], 0);
+        }
+    }
+    if (rc == SBP_OK) rc = cuda_status(time_update(s->d_inst, s->d_active, s->ninst, s->stream), "time update");
+    cudaGraph_t graph = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(s->stream, &graph);
+    if (rc != SBP_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    SBP_TRY_CUDA(ee);
+    s->graph = graph;
+    SBP_TRY_CUDA(cudaGraphInstantiate(&s->gexec, graph, 0));
+    s->sched_dirty = false;
+    return SBP_OK;
+}
+
+sbp_status check_status(sbp_system* s) {
+    unsigned hs = 0;
+    SBP_TRY_CUDA(cudaMemcpyAsync(&hs, s->status, sizeof hs, cudaMemcpyDeviceToHost, s->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(s->st()));
+    if (hs) {
+        set_error("non-physical state detected on device (flags 0x%x: 1 rho<=0, 2 p<=0, 4 detJ<=0)", hs);
+        return SBP_ERR_NONPHYSICAL;
+    }
+    return SBP_OK;
+}
+
+sbp_status run_steps(sbp_system* s, int64_t n) {
+    if (s->sched_dirty) SBP_TRY(build_schedule(s));
+    for (int64_t i = 0; i < n; ++i) SBP_TRY_CUDA(cudaGraphLaunch(s->gexec, s->st()));
+    return SBP_OK;
+}
+
+bool valid_block(const sbp_system* s, int b) { return b >= 0 && b < s->nblocks; }
+
+}  // namespace
+
+extern "C" {
+
+sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nblocks, int ninstances, int precision,
+                             double gamma, sbp_system** out) {
+    clear_error();
+    if (!out || !blocks || nblocks <= 0 || ninstances <= 0 || nblocks > 65535) {
+        set_error("bad arguments (need 1..65535 blocks and at least one instance)");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    if (precision != SBP_PRECISION_F64 && precision != SBP_PRECISION_F32_COMPENSATED) {
+        set_error("unknown precision %d", precision);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device");
+        return SBP_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+        set_error("device %d out of range", device);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    // validate blocks
+    for (int b = 0; b < nblocks; ++b) {
+        const sbp_block_desc& D = blocks[b];
+        OpInfo ox, oy;
+        if (!op_info(D.op_xi, ox) || !op_info(D.op_eta, oy)) {
+            set_error("block %d: unknown operator", b);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        if (!D.x || !D.y) {
+            set_error("block %d: null grid", b);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        if (D.nx < 2 * ox.M || D.nx < ox.N || D.ny < 2 * oy.M || D.ny < oy.N || D.nx * D.ny > (int64_t)1 << 30) {
+            set_error("block %d: %lld x %lld grid does not fit the operators (n >= max(2M, N))", b, (long long)D.ny,
+                      (long long)D.nx);
+            return SBP_ERR_SHAPE;
+        }
+        if (D.instance < 0 || D.instance >= ninstances) {
+            set_error("block %d: instance %d out of range", b, D.instance);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        for (int d = 0; d < 4; ++d) {
+            const int k = D.bc_kind[d];
+            if (k != SBP_BC_THIS && k != SBP_BC_GRID && k != SBP_BC_VORTEX) {
+                set_error("block %d: unknown boundary kind %d", b, k);
+                return SBP_ERR_INVALID_ARGUMENT;
+            }
+            if (k == SBP_BC_GRID) {
+                const int g = D.bc_neighbour[d];
+                if (g < 0 || g >= nblocks) {
+                    set_error("block %d: neighbour %d out of range", b, g);
+                    return SBP_ERR_INVALID_ARGUMENT;
+                }
+                const bool ns = d == SBP_NORTH || d == SBP_SOUTH;
+                const int64_t mine = ns ? D.nx : D.ny, theirs = ns ? blocks[g].nx : blocks[g].ny;
+                if (mine != theirs) {
+                    // SAT_characteristic asserts equal shapes (euler/src/lib.rs:1163)
+                    set_error("block %d: interface with block %d has %lld vs %lld points", b, g, (long long)mine,
+                              (long long)theirs);
+                    return SBP_ERR_SHAPE;
+                }
+                if (blocks[g].instance != D.instance) {
+                    set_error("block %d: neighbour %d belongs to another instance", b, g);
+                    return SBP_ERR_INVALID_ARGUMENT;
+                }
+            }
+        }
+    }
+    sbp_system* s = new sbp_system();
+    s->device = device;
+    s->prec = precision;
+    s->gamma = gamma;
+    s->nblocks = nblocks;
+    s->ninst = ninstances;
+    auto fail = [&](sbp_status st) {
+        destroy_all(s);
+        return st;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_status(cudaSetDevice(device), "cudaSetDevice"));
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    s->num_sms = v > 0 ? v : 148;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    s->smem_optin = v > 0 ? (size_t)v : 48 * 1024;
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(cuda_status(e, "stream"));
+        e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+        if (e != cudaSuccess) return fail(cuda_status(e, "event"));
+    }
+    // layout
+    s->hb.resize(nblocks);
+    s->dense_off.resize(nblocks);
+    s->hoff.resize(nblocks);
+    int64_t hw_total = 0;
+    for (int b = 0; b < nblocks; ++b) {
+        const sbp_block_desc& D = blocks[b];
+        BlockDev& B = s->hb[b];
+        std::memset(&B, 0, sizeof B);
+        OpInfo ox, oy;
+        op_info(D.op_xi, ox);
+        op_info(D.op_eta, oy);
+        B.nx = (int)D.nx;
+        B.ny = (int)D.ny;
+        const int64_t n = D.nx * D.ny;
+        B.npad = (int)pad64(n);
+        B.op_xi = D.op_xi;
+        B.op_eta = D.op_eta;
+        B.instance = D.instance;
+        B.simd_f64 = (int)(8 * (D.nx / 8));
+        B.simd_f32 = (int)(16 * (D.nx / 16));
+        for (int d = 0; d < 4; ++d) {
+            B.bc_kind[d] = D.bc_kind[d];
+            B.bc_nb[d] = D.bc_kind[d] == SBP_BC_GRID ? D.bc_neighbour[d] : b;
+        }
+        B.q_off = s->nq;
+        B.m_off = s->nm;
+        B.x_off = s->nx2;
+        s->nq += 4 * (int64_t)B.npad;
+        s->nm += 5 * (int64_t)B.npad;
+        s->nx2 += 2 * (int64_t)B.npad;
+        B.idx_xi = inv_spacing<double>(ox.h2, D.nx);
+        B.idx_eta = inv_spacing<double>(oy.h2, D.ny);
+        B.idx_xi_f = inv_spacing<float>(ox.h2, D.nx);
+        B.idx_eta_f = inv_spacing<float>(oy.h2, D.ny);
+        // SAT_north/.. penalties: (n-1)/H_0, or (n-2)/H_0 for h2 (euler/src/lib.rs:1033-1037, 1093-1097)
+        B.hi_eta = (oy.h2 ? double(D.ny - 2) : double(D.ny - 1)) / op_h_weights(D.op_eta)[0];
+        B.hi_xi = (ox.h2 ? double(D.nx - 2) : double(D.nx - 1)) / op_h_weights(D.op_xi)[0];
+        s->max_points = std::max(s->max_points, n);
+        s->dense_off[b] = s->dense_total;
+        s->dense_total += 4 * n;
+        s->hoff[b] = hw_total;
+        hw_total += D.nx + D.ny;
+    }
+    s->hi.assign(ninstances, InstanceDev{});
+    for (auto& I : s->hi) {
+        std::memset(&I, 0, sizeof I);
+        set_dt_host(I, NAN);
+        I.time = 0.0;
+        I.mach = 0.5;
+    }
+    s->active.assign(ninstances, 1);
+    // allocations
+    const size_t ts = s->tsize();
+    auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes < 16 ? 16 : bytes); };
+    cudaError_t e = cudaSuccess;
+    e = e ?: alloc((void**)&s->d_blocks, nblocks * sizeof(BlockDev));
+    e = e ?: alloc((void**)&s->d_inst, ninstances * sizeof(InstanceDev));
+    e = e ?: alloc((void**)&s->d_active, ninstances * sizeof(int));
+    e = e ?: alloc(&s->prev_hi, s->nq * ts);
+    e = e ?: alloc(&s->acc_hi, s->nq * ts);
+    e = e ?: alloc(&s->uA, s->nq * ts);
+    e = e ?: alloc(&s->uB, s->nq * ts);
+    if (precision == SBP_PRECISION_F32_COMPENSATED) {
+        e = e ?: alloc(&s->prev_lo, s->nq * ts);
+        e = e ?: alloc(&s->acc_lo, s->nq * ts);
+        e = e ?: alloc((void**)&s->met32, s->nm * sizeof(float));
+    }
+    e = e ?: alloc((void**)&s->met64, s->nm * sizeof(double));
+    e = e ?: alloc((void**)&s->xy, s->nx2 * sizeof(double));
+    e = e ?: alloc((void**)&s->hw, hw_total * sizeof(double));
+    e = e ?: alloc((void**)&s->d_hoff, nblocks * sizeof(int64_t));
+    e = e ?: alloc((void**)&s->d_poff4, nblocks * sizeof(int64_t));
+    e = e ?: alloc((void**)&s->d_poff8, nblocks * sizeof(int64_t));
+    e = e ?: alloc((void**)&s->d_zero, sizeof(int64_t));
+    s->staging_bytes = (size_t)s->dense_total * sizeof(double);
+    e = e ?: alloc(&s->staging, s->staging_bytes);
+    e = e ?: alloc((void**)&s->status, sizeof(unsigned));
+    e = e ?: alloc((void**)&s->d_sums, nblocks * sizeof(double));
+    e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
+    if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
+    cudaStream_t st = s->stream;
+    e = e ?: cudaMemsetAsync(s->prev_hi, 0, s->nq * ts, st);
+    e = e ?: cudaMemsetAsync(s->acc_hi, 0, s->nq * ts, st);
+    e = e ?: cudaMemsetAsync(s->uA, 0, s->nq * ts, st);
+    e = e ?: cudaMemsetAsync(s->uB, 0, s->nq * ts, st);
+    if (s->prev_lo) e = e ?: cudaMemsetAsync(s->prev_lo, 0, s->nq * ts, st);
+    if (s->acc_lo) e = e ?: cudaMemsetAsync(s->acc_lo, 0, s->nq * ts, st);
+    e = e ?: cudaMemsetAsync(s->met64, 0, s->nm * sizeof(double), st);
+    e = e ?: cudaMemsetAsync(s->status, 0, sizeof(unsigned), st);
+    e = e ?: cudaMemsetAsync(s->d_zero, 0, sizeof(int64_t), st);
+    e = e ?: cudaMemcpyAsync(s->d_blocks, s->hb.data(), nblocks * sizeof(BlockDev), cudaMemcpyHostToDevice, st);
+    e = e ?: cudaMemcpyAsync(s->d_inst, s->hi.data(), ninstances * sizeof(InstanceDev), cudaMemcpyHostToDevice, st);
+    e = e ?: cudaMemcpyAsync(s->d_hoff, s->hoff.data(), nblocks * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    {
+        std::vector<int64_t> p8(nblocks);
+        for (int b = 0; b < nblocks; ++b) p8[b] = 2 * s->dense_off[b];
+        e = e ?: cudaMemcpyAsync(s->d_poff4, s->dense_off.data(), nblocks * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                 st);
+        e = e ?: cudaMemcpyAsync(s->d_poff8, p8.data(), nblocks * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    }
+    // H-norm weights per block: hx then hy (euler/src/lib.rs:391-420)
+    {
+        std::vector<double> w(hw_total);
+        for (int b = 0; b < nblocks; ++b) {
+            const sbp_block_desc& D = blocks[b];
+            double* hx = w.data() + s->hoff[b];
+            double* hy = hx + D.nx;
+            for (int dir = 0; dir < 2; ++dir) {
+                const int op = dir == 0 ? D.op_xi : D.op_eta;
+                const int64_t n = dir == 0 ? D.nx : D.ny;
+                double* h = dir == 0 ? hx : hy;
+                OpInfo oi;
+                op_info(op, oi);
+                const double* hw = op_h_weights(op);
+                const double factor = oi.h2 ? 1.0 / double(n - 2) : 1.0 / double(n - 1);
+                for (int64_t i = 0; i < n; ++i) h[i] = 1.0;
+                for (int i = 0; i < oi.M; ++i) {
+                    h[i] = hw[i];
+                    h[n - 1 - i] = hw[i];
+                }
+                for (int64_t i = 0; i < n; ++i) h[i] = h[i] * factor;
+            }
+        }
+        e = e ?: cudaMemcpyAsync(s->hw, w.data(), hw_total * sizeof(double), cudaMemcpyHostToDevice, st);
+        e = e ?: cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) return fail(cuda_status(e, "system setup"));
+    // grids and metrics (Metrics::new per block, in f64)
+    double* tmp = static_cast<double*>(s->staging);  // >= 4 * max_points doubles
+    for (int b = 0; b < nblocks && e == cudaSuccess; ++b) {
+        const sbp_block_desc& D = blocks[b];
+        const BlockDev& B = s->hb[b];
+        const int64_t n = D.nx * D.ny;
+        double* x = s->xy + B.x_off;
+        double* y = x + B.npad;
+        e = e ?: cudaMemcpyAsync(x, D.x, n * sizeof(double), cudaMemcpyHostToDevice, st);
+        e = e ?: cudaMemcpyAsync(y, D.y, n * sizeof(double), cudaMemcpyHostToDevice, st);
+        e = e ?: op_apply(D.op_xi, 0, 0, 0, x, tmp, D.ny, D.nx, 1, n, st);
+        e = e ?: op_apply(D.op_eta, 1, 0, 0, x, tmp + n, D.ny, D.nx, 1, n, st);
+        e = e ?: op_apply(D.op_xi, 0, 0, 0, y, tmp + 2 * n, D.ny, D.nx, 1, n, st);
+        e = e ?: op_apply(D.op_eta, 1, 0, 0, y, tmp + 3 * n, D.ny, D.nx, 1, n, st);
+        e = e ?: metrics_combine(tmp, tmp + n, tmp + 2 * n, tmp + 3 * n, n, s->met64 + B.m_off, B.npad, s->status, st);
+    }
+    if (e == cudaSuccess && s->met32) e = narrow_f32(s->met64, s->met32, s->nm, st);
+    if (e != cudaSuccess) return fail(cuda_status(e, "metrics"));
+    sbp_status cs = check_status(s);
+    if (cs != SBP_OK) {
+        set_error("non-positive Jacobian determinant in the grid (Metrics::new asserts detj > 0)");
+        return fail(cs);
+    }
+    // every operator pair must be available
+    for (int b = 0; b < nblocks; ++b) {
+        OpInfo ox, oy;
+        op_info(s->hb[b].op_xi, ox);
+        op_info(s->hb[b].op_eta, oy);
+        if (!stage_kernel_ptr(s->prec, s->hb[b].op_xi, s->hb[b].op_eta, ox.upwind && oy.upwind)) {
+            set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", s->hb[b].op_xi,
+                      s->hb[b].op_eta);
+            return fail(SBP_ERR_UNSUPPORTED);
+        }
+    }
+    *out = s;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_destroy(sbp_system* sys) {
+    clear_error();
+    destroy_all(sys);
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_force_trad(sbp_system* sys, int force_trad) {
+    clear_error();
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    if (sys->force_trad != (force_trad != 0)) {
+        sys->force_trad = force_trad != 0;
+        sys->sched_dirty = true;
+    }
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_vortex(sbp_system* sys, int instance, const sbp_vortex_params* vp) {
+    clear_error();
+    if (!sys || !vp || instance >= sys->ninst || vp->nvortices < 0 || vp->nvortices > 5) {
+        set_error("bad vortex parameters / instance");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(sys->device);
+    SBP_TRY(sync_times(sys));
+    for (int i = 0; i < sys->ninst; ++i) {
+        if (instance >= 0 && i != instance) continue;
+        InstanceDev& I = sys->hi[i];
+        I.nvort = vp->nvortices;
+        for (int k = 0; k < 5; ++k) {
+            I.x0[k] = vp->x0[k];
+            I.y0[k] = vp->y0[k];
+            I.rstar[k] = vp->rstar[k];
+            I.eps[k] = vp->eps[k];
+        }
+        I.mach = vp->mach;
+    }
+    return upload_instances(sys);
+}
+
+sbp_status sbp_system_init_vortex(sbp_system* sys, int instance, double t) {
+    clear_error();
+    if (!sys || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    SBP_TRY_CUDA(vortex_init(sys->d_blocks, sys->d_inst, sys->nblocks, instance, sys->gamma, t, sys->xy, sys->prec,
+                             sys->prev_hi, sys->prev_lo, sys->max_points, sys->st()));
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), sys->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(sys->st()));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_state(sbp_system* sys, int block, const double* q) {
+    clear_error();
+    if (!sys || !q || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    const BlockDev& B = sys->hb[block];
+    const int64_t n = (int64_t)B.nx * B.ny;
+    cudaStream_t st = sys->st();
+    if (sys->prec == 0) {
+        SBP_TRY_CUDA(cudaMemcpy2DAsync(static_cast<double*>(sys->prev_hi) + B.q_off, B.npad * sizeof(double), q,
+                                       n * sizeof(double), n * sizeof(double), 4, cudaMemcpyHostToDevice, st));
+    } else {
+        SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+        SBP_TRY_CUDA(unpack_state(sys->d_blocks + block, 1, sys->d_zero, sys->prec, 0, sys->staging, sys->prev_hi,
+                                  sys->prev_lo, n, st));
+    }
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_get_state(sbp_system* sys, int block, double* q) {
+    clear_error();
+    if (!sys || !q || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    const BlockDev& B = sys->hb[block];
+    const int64_t n = (int64_t)B.nx * B.ny;
+    cudaStream_t st = sys->st();
+    if (sys->prec == 0) {
+        SBP_TRY_CUDA(cudaMemcpy2DAsync(q, n * sizeof(double), static_cast<double*>(sys->prev_hi) + B.q_off,
+                                       B.npad * sizeof(double), n * sizeof(double), 4, cudaMemcpyDeviceToHost, st));
+    } else {
+        SBP_TRY_CUDA(pack_state(sys->d_blocks + block, 1, sys->d_zero, sys->prec, 0, sys->prev_hi, sys->prev_lo,
+                                sys->staging, n, st));
+        SBP_TRY_CUDA(cudaMemcpyAsync(q, sys->staging, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    return SBP_OK;
+}
+
+int64_t sbp_system_state_count(const sbp_system* sys, int dtype) {
+    if (!sys) return -1;
+    return dtype == SBP_F32 ? 2 * sys->dense_total : sys->dense_total;
+}
+
+sbp_status sbp_system_set_state_all(sbp_system* sys, int dtype, const void* q) {
+    clear_error();
+    if (!sys || !q || (dtype != SBP_F64 && dtype != SBP_F32)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    const size_t bytes = (size_t)sys->dense_total * (dtype == SBP_F64 ? 8 : 8);
+    SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, bytes, cudaMemcpyHostToDevice, st));
+    SBP_TRY_CUDA(unpack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+                              dtype, sys->staging, sys->prev_hi, sys->prev_lo, sys->max_points, st));
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q) {
+    clear_error();
+    if (!sys || !q || (dtype != SBP_F64 && dtype != SBP_F32)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    const size_t bytes = (size_t)sys->dense_total * 8;
+    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+                            dtype, sys->prev_hi, sys->prev_lo, sys->staging, sys->max_points, st));
+    SBP_TRY_CUDA(cudaMemcpyAsync(q, sys->staging, bytes, cudaMemcpyDeviceToHost, st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_dt(sbp_system* sys, int instance, double dt) {
+    clear_error();
+    if (!sys || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    SBP_TRY(sync_times(sys));
+    for (int i = 0; i < sys->ninst; ++i)
+        if (instance < 0 || i == instance) set_dt_host(sys->hi[i], dt);
+    SBP_TRY(upload_instances(sys));
+    SBP_TRY_CUDA(cudaStreamSynchronize(sys->st()));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_time(sbp_system* sys, int instance, double t) {
+    clear_error();
+    if (!sys || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    SBP_TRY(sync_times(sys));
+    for (int i = 0; i < sys->ninst; ++i)
+        if (instance < 0 || i == instance) sys->hi[i].time = t;
+    SBP_TRY(upload_instances(sys));
+    SBP_TRY_CUDA(cudaStreamSynchronize(sys->st()));
+    return SBP_OK;
+}
+
+sbp_status sbp_system_get_time(sbp_system* sys, int instance, double* t) {
+    clear_error();
+    if (!sys || !t || instance < 0 || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    SBP_TRY(sync_times(sys));
+    *t = sys->hi[instance].time;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_max_dt(sbp_system* sys, int instance, double* dt) {
+    clear_error();
+    if (!sys || !dt || instance < 0 || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->d_speeds, 0, 2 * sys->nblocks * sizeof(unsigned long long), st));
+    SBP_TRY_CUDA(max_speeds(sys->d_blocks, sys->nblocks, sys->prec, sys->prev_hi, sys->met64, sys->max_points,
+                            sys->d_speeds, st));
+    std::vector<unsigned long long> sp(2 * sys->nblocks);
+    SBP_TRY_CUDA(cudaMemcpyAsync(sp.data(), sys->d_speeds, sp.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    bool is_h2 = false;
+    for (const auto& B : sys->hb) {
+        if (B.instance != instance) continue;
+        OpInfo ox, oy;
+        op_info(B.op_xi, ox);
+        op_info(B.op_eta, oy);
+        is_h2 = is_h2 || ox.h2 || oy.h2;
+    }
+    const double c_max = is_h2 ? 0.5 : 1.0;
+    double max_dt = INFINITY;
+    for (int b = 0; b < sys->nblocks; ++b) {
+        const BlockDev& B = sys->hb[b];
+        if (B.instance != instance) continue;
+        double mu, mv;
+        std::memcpy(&mu, &sp[2 * b], 8);
+        std::memcpy(&mv, &sp[2 * b + 1], 8);
+        const double dx = 1.0 / double(B.nx), dy = 1.0 / double(B.ny);
+        const double c_dt = std::fmax(mu / dx, mv / dy);
+        max_dt = std::fmin(max_dt, c_max / c_dt);
+    }
+    *dt = max_dt;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_advance(sbp_system* sys, int64_t nsteps) {
+    clear_error();
+    if (!sys || nsteps < 0) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    for (int i = 0; i < sys->ninst; ++i)
+        if (!(sys->hi[i].dt == sys->hi[i].dt)) {
+            set_error("instance %d has no dt (call sbp_system_set_dt first)", i);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+    bool all = true;
+    for (int a : sys->active) all = all && a;
+    if (!all) {
+        std::fill(sys->active.begin(), sys->active.end(), 1);
+        sys->sched_dirty = true;
+    }
+    SBP_TRY(run_steps(sys, nsteps));
+    return check_status(sys);
+}
+
+sbp_status sbp_system_advance_instances(sbp_system* sys, const int64_t* nsteps) {
+    clear_error();
+    if (!sys || !nsteps) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    std::vector<int64_t> left(nsteps, nsteps + sys->ninst);
+    for (int i = 0; i < sys->ninst; ++i) {
+        if (left[i] < 0) return SBP_ERR_INVALID_ARGUMENT;
+        if (left[i] > 0 && !(sys->hi[i].dt == sys->hi[i].dt)) {
+            set_error("instance %d has no dt", i);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+    }
+    for (;;) {
+        int64_t seg = INT64_MAX;
+        std::vector<int> act(sys->ninst, 0);
+        for (int i = 0; i < sys->ninst; ++i)
+            if (left[i] > 0) {
+                act[i] = 1;
+                seg = std::min(seg, left[i]);
+            }
+        if (seg == INT64_MAX) break;
+        if (act != sys->active) {
+            sys->active = act;
+            sys->sched_dirty = true;
+        }
+        SBP_TRY(run_steps(sys, seg));
+        for (int i = 0; i < sys->ninst; ++i)
+            if (act[i]) left[i] -= seg;
+    }
+    return check_status(sys);
+}
+
+sbp_status sbp_system_error(sbp_system* sys, double* per_instance) {
+    clear_error();
+    if (!sys || !per_instance) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sys->nblocks * sizeof(double), st));
+    SBP_TRY_CUDA(error_terms(sys->d_blocks, sys->d_inst, sys->nblocks, sys->gamma, sys->xy, sys->prec, sys->prev_hi,
+                             sys->prev_lo, sys->hw, sys->d_hoff, sys->max_points, sys->d_sums, st));
+    std::vector<double> sums(sys->nblocks);
+    SBP_TRY_CUDA(cudaMemcpyAsync(sums.data(), sys->d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < sys->ninst; ++i) per_instance[i] = 0.0;
+    for (int b = 0; b < sys->nblocks; ++b) per_instance[sys->hb[b].instance] += std::sqrt(sums[b]);
+    return SBP_OK;
+}
+
+sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double* err) {
+    clear_error();
+    if (!sys || !q || !err || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    const BlockDev& B = sys->hb[block];
+    const int64_t n = (int64_t)B.nx * B.ny;
+    SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sizeof(double), st));
+    const double* hx = sys->hw + sys->hoff[block];
+    SBP_TRY_CUDA(diff_terms(sys->d_blocks + block, sys->prec, sys->prev_hi, sys->prev_lo,
+                            static_cast<const double*>(sys->staging), hx, hx + B.nx, n, sys->d_sums, st));
+    double s = 0;
+    SBP_TRY_CUDA(cudaMemcpyAsync(&s, sys->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    *err = std::sqrt(s);
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_tiles(sbp_system* sys, int ty, int tx, int threads) {
+    clear_error();
+    if (!sys || ty < 8 || tx < 8 || ty > 256 || tx > 256) {
+        set_error("tile dimensions must be within [8, 256]");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    if (threads != 0 && (threads % 32 != 0 || threads > 256 || threads < 32)) {
+        set_error("threads must be a multiple of 32 in [32, 256]");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    sys->TY = ty;
+    sys->TX = tx;
+    if (threads) sys->threads = threads;
+    sys->sched_dirty = true;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads) {
+    clear_error();
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    for (int i = 0; i < sys->ninst; ++i)
+        if (!(sys->hi[i].dt == sys->hi[i].dt)) {
+            set_error("instance %d has no dt", i);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+    std::fill(sys->active.begin(), sys->active.end(), 1);
+    static const int cand[][3] = {{16, 32, 256}, {32, 32, 256}, {16, 64, 256}, {32, 64, 256},
+                                  {8, 64, 256},  {64, 32, 256}, {8, 32, 128},  {16, 16, 128}};
+    const size_t ts = sys->tsize();
+    // save state and times
+    void* save_hi = nullptr;
+    void* save_lo = nullptr;
+    SBP_TRY_CUDA(cudaMalloc(&save_hi, sys->nq * ts));
+    if (sys->prev_lo) SBP_TRY_CUDA(cudaMalloc(&save_lo, sys->nq * ts));
+    cudaStream_t st = sys->st();
+    SBP_TRY(sync_times(sys));
+    std::vector<InstanceDev> save_inst = sys->hi;
+    cudaMemcpyAsync(save_hi, sys->prev_hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
+    if (save_lo) cudaMemcpyAsync(save_lo, sys->prev_lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int bi = -1;
+    const int oTY = sys->TY, oTX = sys->TX, oth = sys->threads;
+    for (int c = 0; c < (int)(sizeof cand / sizeof cand[0]); ++c) {
+        sys->TY = cand[c][0];
+        sys->TX = cand[c][1];
+        sys->threads = cand[c][2];
+        sys->sched_dirty = true;
+        if (build_schedule(sys) != SBP_OK) continue;
+        if (run_steps(sys, 1) != SBP_OK) continue;
+        const int reps = 3;
+        cudaEventRecord(e0, st);
+        if (run_steps(sys, reps) != SBP_OK) continue;
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            bi = c;
+        }
+    }
+    // restore
+    cudaMemcpyAsync(sys->prev_hi, save_hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
+    if (save_lo) cudaMemcpyAsync(sys->prev_lo, save_lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
+    sys->hi = save_inst;
+    upload_instances(sys);
+    cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st);
+    cudaStreamSynchronize(st);
+    cudaFree(save_hi);
+    if (save_lo) cudaFree(save_lo);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    clear_error();
+    if (bi < 0) {
+        sys->TY = oTY;
+        sys->TX = oTX;
+        sys->threads = oth;
+        sys->sched_dirty = true;
+        set_error("no tile candidate could run");
+        return SBP_ERR_CUDA;
+    }
+    sys->TY = cand[bi][0];
+    sys->TX = cand[bi][1];
+    sys->threads = cand[bi][2];
+    sys->sched_dirty = true;
+    if (ty) *ty = sys->TY;
+    if (tx) *tx = sys->TX;
+    if (threads) *threads = sys->threads;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_set_stream(sbp_system* sys, void* stream) {
+    clear_error();
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    sys->user_stream = static_cast<cudaStream_t>(stream);
+    sys->has_user_stream = stream != nullptr;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q) {
+    clear_error();
+    if (!sys || !d_q || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
+    *d_q = static_cast<char*>(sys->prev_hi) + sys->hb[block].q_off * sys->tsize();
+    return SBP_OK;
+}
+
+int sbp_system_launches_per_step(const sbp_system* sys) {
+    if (!sys) return -1;
+    if (sys->sched_dirty) {
+        // count the operator pairs present without building
+        std::vector<std::pair<int, int>> pairs;
+        for (const auto& B : sys->hb) {
+            if (!sys->active[B.instance]) continue;
+            auto p = std::make_pair(B.op_xi, B.op_eta);
+            if (std::find(pairs.begin(), pairs.end(), p) == pairs.end()) pairs.push_back(p);
+        }
+        return 4 * (int)pairs.size() + 1;
+    }
+    return 4 * (int)sys->groups.size() + 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,295 @@
+// System-level kernels: metric assembly, vortex data, error norms, CFL speeds, time update and
+// state packing.  Compiled with -fmad=false so the f64 arithmetic matches the reference's.
+#include <cuda_runtime.h>
+
+#include "system_kernels.h"
+
+namespace sbp {
+
+namespace {
+
+constexpr int kT = 256;
+
+__global__ void metrics_combine_kernel(const double* __restrict__ x_xi, const double* __restrict__ x_eta,
+                                       const double* __restrict__ y_xi, const double* __restrict__ y_eta, int64_t n,
+                                       double* __restrict__ out, int64_t ps, unsigned* status) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double a = x_xi[i], b = x_eta[i], c = y_xi[i], d = y_eta[i];
+        const double detj = a * d - b * c;
+        if (!(detj > 0.0)) atomicOr(status, STATUS_DETJ);
+        out[i] = detj;
+        out[ps + i] = d;
+        out[2 * ps + i] = -b;
+        out[3 * ps + i] = -c;
+        out[4 * ps + i] = a;
+    }
+}
+
+__global__ void narrow_kernel(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = float(in[i]);
+}
+
+__device__ __forceinline__ void split_f32(double v, float& hi, float& lo) {
+    hi = float(v);
+    lo = float(v - double(hi));
+}
+
+__global__ void vortex_init_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst,
+                                   int instance, double gamma, double t, const double* __restrict__ xy, int prec,
+                                   void* q_hi, void* q_lo) {
+    const BlockDev& B = blocks[blockIdx.y];
+    if (instance >= 0 && B.instance != instance) return;
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    const InstanceDev& I = inst[B.instance];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double q[4];
+        vortex_point(I, gamma, t, xy[B.x_off + i], xy[B.x_off + np + i], q);
+        for (int c = 0; c < 4; ++c) {
+            const int64_t g = B.q_off + c * np + i;
+            if (prec == 0) {
+                static_cast<double*>(q_hi)[g] = q[c];
+            } else {
+                float h, l;
+                split_f32(q[c], h, l);
+                static_cast<float*>(q_hi)[g] = h;
+                static_cast<float*>(q_lo)[g] = l;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ double state_at(int prec, const void* q_hi, const void* q_lo, int64_t g) {
+    if (prec == 0) return static_cast<const double*>(q_hi)[g];
+    return double(static_cast<const float*>(q_hi)[g]) + double(static_cast<const float*>(q_lo)[g]);
+}
+
+__global__ void error_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst, double gamma,
+                             const double* __restrict__ xy, int prec, const void* q_hi, const void* q_lo,
+                             const double* __restrict__ hw, const int64_t* __restrict__ h_off,
+                             double* __restrict__ sums) {
+    const int b = blockIdx.y;
+    const BlockDev& B = blocks[b];
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    const InstanceDev& I = inst[B.instance];
+    const double* hx = hw + h_off[b];
+    const double* hy = hx + B.nx;
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)(i / B.nx), col = (int)(i - (int64_t)row * B.nx);
+        double v[4];
+        vortex_point(I, gamma, I.time, xy[B.x_off + i], xy[B.x_off + np + i], v);
+        for (int c = 0; c < 4; ++c) {
+            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i) - v[c];
+            s += d * d * hx[col] * hy[row];
+        }
+    }
+    // block reduction
+    __shared__ double red[kT / 32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (kT / 32) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(sums + b, s);
+    }
+}
+
+__global__ void diff_kernel(const BlockDev* __restrict__ blk, int prec, const void* q_hi, const void* q_lo,
+                            const double* __restrict__ dense, const double* __restrict__ hx,
+                            const double* __restrict__ hy, double* __restrict__ sum) {
+    const BlockDev& B = *blk;
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)(i / B.nx), col = (int)(i - (int64_t)row * B.nx);
+        for (int c = 0; c < 4; ++c) {
+            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i) - dense[c * n + i];
+            s += d * d * hx[col] * hy[row];
+        }
+    }
+    __shared__ double red[kT / 32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (kT / 32) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(sum, s);
+    }
+}
+
+__global__ void max_speed_kernel(const BlockDev* __restrict__ blocks, int prec, const void* q_hi,
+                                 const double* __restrict__ met64, unsigned long long* out) {
+    const int b = blockIdx.y;
+    const BlockDev& B = blocks[b];
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    double mu = 0.0, mv = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double rho, rhou, rhov;
+        if (prec == 0) {
+            const double* q = static_cast<const double*>(q_hi) + B.q_off;
+            rho = q[i];
+            rhou = q[np + i];
+            rhov = q[2 * np + i];
+        } else {
+            const float* q = static_cast<const float*>(q_hi) + B.q_off;
+            rho = q[i];
+            rhou = q[np + i];
+            rhov = q[2 * np + i];
+        }
+        const double* m = met64 + B.m_off;
+        const double u = rhou / rho, v = rhov / rho;
+        const double uhat = m[np + i] * u + m[2 * np + i] * v;
+        const double vhat = m[3 * np + i] * u + m[4 * np + i] * v;
+        mu = fmax(mu, fabs(uhat));
+        mv = fmax(mv, fabs(vhat));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = fmax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+        mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        // non-negative doubles order like their bit patterns
+        atomicMax(out + 2 * b, (unsigned long long)__double_as_longlong(mu));
+        atomicMax(out + 2 * b + 1, (unsigned long long)__double_as_longlong(mv));
+    }
+}
+
+__global__ void time_update_kernel(InstanceDev* inst, const int* __restrict__ active, int ninst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ninst && active[i]) inst[i].time = inst[i].time + inst[i].dt;
+}
+
+__global__ void pack_kernel(const BlockDev* __restrict__ blocks, const int64_t* __restrict__ poff, int prec,
+                            int dtype, const void* q_hi, const void* q_lo, void* packed) {
+    const BlockDev& B = blocks[blockIdx.y];
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    const int64_t o = poff[blockIdx.y];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < 4; ++c) {
+            const int64_t g = B.q_off + c * np + i;
+            if (dtype == 0) {
+                static_cast<double*>(packed)[o + c * n + i] = state_at(prec, q_hi, q_lo, g);
+            } else {
+                float* p = static_cast<float*>(packed) + o;
+                if (prec == 0) {
+                    float h, l;
+                    split_f32(static_cast<const double*>(q_hi)[g], h, l);
+                    p[c * n + i] = h;
+                    p[4 * n + c * n + i] = l;
+                } else {
+                    p[c * n + i] = static_cast<const float*>(q_hi)[g];
+                    p[4 * n + c * n + i] = static_cast<const float*>(q_lo)[g];
+                }
+            }
+        }
+    }
+}
+
+__global__ void unpack_kernel(const BlockDev* __restrict__ blocks, const int64_t* __restrict__ poff, int prec,
+                              int dtype, const void* packed, void* q_hi, void* q_lo) {
+    const BlockDev& B = blocks[blockIdx.y];
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    const int64_t o = poff[blockIdx.y];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < 4; ++c) {
+            const int64_t g = B.q_off + c * np + i;
+            double v;
+            if (dtype == 0) {
+                v = static_cast<const double*>(packed)[o + c * n + i];
+            } else {
+                const float* p = static_cast<const float*>(packed) + o;
+                v = double(p[c * n + i]) + double(p[4 * n + c * n + i]);
+            }
+            if (prec == 0) {
+                static_cast<double*>(q_hi)[g] = v;
+            } else if (dtype == 1) {
+                const float* p = static_cast<const float*>(packed) + o;
+                static_cast<float*>(q_hi)[g] = p[c * n + i];
+                static_cast<float*>(q_lo)[g] = p[4 * n + c * n + i];
+            } else {
+                float h, l;
+                split_f32(v, h, l);
+                static_cast<float*>(q_hi)[g] = h;
+                static_cast<float*>(q_lo)[g] = l;
+            }
+        }
+    }
+}
+
+dim3 per_block_grid(int nblocks, int64_t max_points) {
+    int64_t gx = (max_points + kT - 1) / kT;
+    if (gx > 1024) gx = 1024;
+    if (gx < 1) gx = 1;
+    return dim3((unsigned)gx, (unsigned)nblocks, 1);
+}
+
+int flat_grid(int64_t n) {
+    int64_t g = (n + kT - 1) / kT;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+cudaError_t metrics_combine(const double* x_xi, const double* x_eta, const double* y_xi, const double* y_eta,
+                            int64_t n, double* out, int64_t pstride, unsigned* status, cudaStream_t st) {
+    metrics_combine_kernel<<<flat_grid(n), kT, 0, st>>>(x_xi, x_eta, y_xi, y_eta, n, out, pstride, status);
+    return cudaGetLastError();
+}
+
+cudaError_t narrow_f32(const double* in, float* out, int64_t n, cudaStream_t st) {
+    narrow_kernel<<<flat_grid(n), kT, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t vortex_init(const BlockDev* blocks, const InstanceDev* inst, int nblocks, int instance, double gamma,
+                        double t, const double* xy, int prec, void* q_hi, void* q_lo, int64_t max_points,
+                        cudaStream_t st) {
+    vortex_init_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, instance, gamma, t, xy, prec,
+                                                                          q_hi, q_lo);
+    return cudaGetLastError();
+}
+
+cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nblocks, double gamma,
+                        const double* xy, int prec, const void* q_hi, const void* q_lo, const double* hweights,
+                        const int64_t* h_off, int64_t max_points, double* block_sums, cudaStream_t st) {
+    error_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, gamma, xy, prec, q_hi, q_lo,
+                                                                    hweights, h_off, block_sums);
+    return cudaGetLastError();
+}
+
+cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
+                       const double* hx, const double* hy, int64_t max_points, double* sum, cudaStream_t st) {
+    diff_kernel<<<per_block_grid(1, max_points).x, kT, 0, st>>>(block, prec, q_hi, q_lo, dense, hx, hy, sum);
+    return cudaGetLastError();
+}
+
+cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
+                       int64_t max_points, unsigned long long* out2, cudaStream_t st) {
+    max_speed_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, prec, q_hi, met64, out2);
+    return cudaGetLastError();
+}
+
+cudaError_t time_update(InstanceDev* inst, const int* active, int ninst, cudaStream_t st) {
+    time_update_kernel<<<(ninst + kT - 1) / kT, kT, 0, st>>>(inst, active, ninst);
+    return cudaGetLastError();
+}
+
+cudaError_t pack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
+                       const void* q_hi, const void* q_lo, void* packed, int64_t max_points, cudaStream_t st) {
+    pack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, packed_off, prec, dtype, q_hi, q_lo,
+                                                                   packed);
+    return cudaGetLastError();
+}
+
+cudaError_t unpack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
+                         const void* packed, void* q_hi, void* q_lo, int64_t max_points, cudaStream_t st) {
+    unpack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, packed_off, prec, dtype, packed, q_hi,
+                                                                     q_lo);
+    return cudaGetLastError();
+}
+
+}  // namespace sbp

@@ -1,0 +1,51 @@
+// Launchers of the system-level kernels (system_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "euler_device.cuh"
+
+namespace sbp {
+
+// Metrics::new combine step (sbp/src/grid.rs:101-130): from the four derivative planes build
+// detj, J dxi/dx = y_eta, J dxi/dy = -x_eta, J deta/dx = -y_xi, J deta/dy = x_xi into `out`
+// (5 planes spaced `pstride`); sets STATUS_DETJ in *status if detj <= 0 anywhere.
+cudaError_t metrics_combine(const double* x_xi, const double* x_eta, const double* y_xi, const double* y_eta,
+                            int64_t n, double* out, int64_t pstride, unsigned* status, cudaStream_t st);
+
+// Narrow f64 planes to f32 (n elements).
+cudaError_t narrow_f32(const double* in, float* out, int64_t n, cudaStream_t st);
+
+// Vortex initial data for every block whose instance is selected (instance < 0: all).
+// f64 state: q_hi only.  f32 state: (hi, lo) split of the f64 value.
+cudaError_t vortex_init(const BlockDev* blocks, const InstanceDev* inst, int nblocks, int instance, double gamma,
+                        double t, const double* xy, int prec, void* q_hi, void* q_lo, int64_t max_points,
+                        cudaStream_t st);
+
+// Field::h2_err terms against the vortex at each block's instance time: block_sums[b] += sum of
+// (q - vortex)^2 hx hy over the block (euler/src/lib.rs:377-431).
+cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nblocks, double gamma,
+                        const double* xy, int prec, const void* q_hi, const void* q_lo, const double* hweights,
+                        const int64_t* h_off, int64_t max_points, double* block_sums, cudaStream_t st);
+
+// Field::h2_err of one block's state against a dense (4, ny, nx) f64 field: *sum += terms.
+cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
+                       const double* hx, const double* hy, int64_t max_points, double* sum, cudaStream_t st);
+
+// max |uhat|, max |vhat| per block (multigrid/src/system.rs:555-580), as ordered bit patterns.
+cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
+                       int64_t max_points, unsigned long long* out2, cudaStream_t st);
+
+// time[i] += dt[i] for the instances whose flag is set.
+cudaError_t time_update(InstanceDev* inst, const int* active, int ninst, cudaStream_t st);
+
+// Packed host layout (blocks concatenated, each (4, ny, nx) dense) <-> padded device planes.
+// dtype of the packed buffer: 0 = f64 (widened / split to hi+lo for f32 state),
+//                              1 = f32 hi planes followed by lo planes per block.
+cudaError_t pack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
+                       const void* q_hi, const void* q_lo, void* packed, int64_t max_points, cudaStream_t st);
+cudaError_t unpack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
+                         const void* packed, void* q_hi, void* q_lo, int64_t max_points, cudaStream_t st);
+
+}  // namespace sbp

@@ -1,0 +1,185 @@
+"""GPU systems of curvilinear blocks (the sbp_system_* C ABI).
+
+`BlockSystem` is the common engine behind the reference-shaped front ends:
+euler.System (one periodic block, euler/src/lib.rs:20-188), multigrid.System (many blocks
+coupled by SATs, multigrid/src/system.rs:368-636) and ensemble.Ensemble (independent
+solves).  A system holds, per block, the grid, its f64 metrics and the RK4 buffers in GPU
+memory; stepping runs fused stage kernels replayed as a CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from ._capi import BC_GRID, BC_THIS, BC_VORTEX, F32, F64, check  # noqa: F401
+from .operators import SbpOperator2d
+
+PRECISIONS = {"f64": _capi.PRECISION_F64, "f32c": _capi.PRECISION_F32_COMPENSATED}
+
+
+@dataclass
+class Vortice:
+    """euler::Vortice (euler/src/vortex.rs:4-10)."""
+    x0: float
+    y0: float
+    rstar: float
+    eps: float
+
+
+@dataclass
+class VortexParameters:
+    """euler::VortexParameters (euler/src/vortex.rs:15-21): up to 5 superposed vortices."""
+    vortices: list = field(default_factory=list)
+    mach: float = 0.5
+
+    def to_c(self) -> _capi.VortexParams:
+        if len(self.vortices) > 5:
+            raise ValueError("at most 5 vortices")
+        vp = _capi.VortexParams()
+        vp.nvortices = len(self.vortices)
+        for i, v in enumerate(self.vortices):
+            vp.x0[i], vp.y0[i], vp.rstar[i], vp.eps[i] = v.x0, v.y0, v.rstar, v.eps
+        vp.mach = self.mach
+        return vp
+
+
+@dataclass
+class BlockSpec:
+    """One block: grid (ny, nx), operator, boundary kinds (N, S, E, W) and instance."""
+    x: np.ndarray
+    y: np.ndarray
+    op: SbpOperator2d
+    bc: list  # 4 x (kind, neighbour)
+    instance: int = 0
+
+
+class BlockSystem:
+    def __init__(self, blocks: list[BlockSpec], ninstances: int = 1, precision: str = "f64", gamma: float = 1.4,
+                 device: int = 0):
+        self.precision = precision
+        self.gamma = gamma
+        self.shapes = []
+        self._keep = []
+        arr = (_capi.BlockDesc * len(blocks))()
+        for i, b in enumerate(blocks):
+            x = np.ascontiguousarray(b.x, dtype=np.float64)
+            y = np.ascontiguousarray(b.y, dtype=np.float64)
+            if x.shape != y.shape or x.ndim != 2:
+                raise ValueError("x and y must be 2-D arrays of the same shape")
+            self._keep += [x, y]
+            arr[i].ny, arr[i].nx = x.shape
+            arr[i].op_xi, arr[i].op_eta = b.op.ids
+            arr[i].x = x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            arr[i].y = y.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            for d in range(4):
+                arr[i].bc_kind[d], arr[i].bc_neighbour[d] = b.bc[d]
+            arr[i].instance = b.instance
+            self.shapes.append(x.shape)
+        self.ninstances = ninstances
+        self.nblocks = len(blocks)
+        self.block_instance = [b.instance for b in blocks]
+        h = ctypes.c_void_p()
+        check(_capi.lib.sbp_system_create(device, arr, len(blocks), ninstances, PRECISIONS[precision], gamma,
+                                          ctypes.byref(h)))
+        self.h = h
+        self._keep = []
+
+    # -- lifecycle
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            _capi.lib.sbp_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- configuration
+    def set_force_trad(self, on: bool) -> None:
+        check(_capi.lib.sbp_system_set_force_trad(self.h, int(on)))
+
+    def set_vortex(self, params: VortexParameters, instance: int = -1) -> None:
+        vp = params.to_c()
+        check(_capi.lib.sbp_system_set_vortex(self.h, instance, ctypes.byref(vp)))
+
+    def init_vortex(self, t: float = 0.0, instance: int = -1) -> None:
+        check(_capi.lib.sbp_system_init_vortex(self.h, instance, t))
+
+    def set_dt(self, dt: float, instance: int = -1) -> None:
+        check(_capi.lib.sbp_system_set_dt(self.h, instance, dt))
+
+    def set_time(self, t: float, instance: int = -1) -> None:
+        check(_capi.lib.sbp_system_set_time(self.h, instance, t))
+
+    def time(self, instance: int = 0) -> float:
+        t = ctypes.c_double()
+        check(_capi.lib.sbp_system_get_time(self.h, instance, ctypes.byref(t)))
+        return t.value
+
+    def set_tiles(self, ty: int, tx: int, threads: int = 0) -> None:
+        check(_capi.lib.sbp_system_set_tiles(self.h, ty, tx, threads))
+
+    def autotune(self) -> tuple[int, int, int]:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(_capi.lib.sbp_system_autotune(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def set_stream(self, stream_handle: int) -> None:
+        check(_capi.lib.sbp_system_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def launches_per_step(self) -> int:
+        return _capi.lib.sbp_system_launches_per_step(self.h)
+
+    # -- state
+    def set_state(self, block: int, q: np.ndarray) -> None:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        if q.shape != (4,) + tuple(self.shapes[block]):
+            raise ValueError(f"state of block {block} must be (4, {self.shapes[block][0]}, {self.shapes[block][1]})")
+        check(_capi.lib.sbp_system_set_state(self.h, block, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def state(self, block: int) -> np.ndarray:
+        q = np.zeros((4,) + tuple(self.shapes[block]))
+        check(_capi.lib.sbp_system_get_state(self.h, block, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return q
+
+    def state_count(self, dtype: int = F64) -> int:
+        return _capi.lib.sbp_system_state_count(self.h, dtype)
+
+    def set_state_all(self, buf, dtype: int = F64) -> None:
+        """buf: host buffer (numpy array or pinned torch tensor) holding every block's state."""
+        ptr = buf.ctypes.data if isinstance(buf, np.ndarray) else buf.data_ptr()
+        check(_capi.lib.sbp_system_set_state_all(self.h, dtype, ctypes.c_void_p(ptr)))
+
+    def get_state_all(self, buf, dtype: int = F64) -> None:
+        ptr = buf.ctypes.data if isinstance(buf, np.ndarray) else buf.data_ptr()
+        check(_capi.lib.sbp_system_get_state_all(self.h, dtype, ctypes.c_void_p(ptr)))
+
+    # -- stepping and diagnostics
+    def max_dt(self, instance: int = 0) -> float:
+        dt = ctypes.c_double()
+        check(_capi.lib.sbp_system_max_dt(self.h, instance, ctypes.byref(dt)))
+        return dt.value
+
+    def advance(self, nsteps: int) -> None:
+        check(_capi.lib.sbp_system_advance(self.h, int(nsteps)))
+
+    def advance_instances(self, nsteps) -> None:
+        arr = (ctypes.c_int64 * self.ninstances)(*[int(n) for n in nsteps])
+        check(_capi.lib.sbp_system_advance_instances(self.h, arr))
+
+    def errors(self) -> np.ndarray:
+        out = np.zeros(self.ninstances)
+        check(_capi.lib.sbp_system_error(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def h2_err(self, block: int, q: np.ndarray) -> float:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        e = ctypes.c_double()
+        check(_capi.lib.sbp_system_h2_err(self.h, block, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          ctypes.byref(e)))
+        return e.value
