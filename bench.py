@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-accuracy", action="store_true")
+    p.add_argument("--tiles", default="", help="TY,TX,THREADS: fixed tile schedule instead of the autotuner")
     return p.parse_args()
 
 
@@ -154,7 +156,7 @@ def cpu_baseline(insts, seconds, nthreads, steps_per_sample=1):
     small = min(insts, key=lambda i: i.side)
     blk = workloads.ensemble_blocks([small])[0]
     s = orc.System([dict(x=blk.x, y=blk.y, op_xi=small.op_id, op_eta=small.op_id, bc=list(blk.bc))], fast=True)
-    s.set_vortex([dict(x0=small.x0, y0=small.y0, rstar=0.5, eps=small.eps)], small.mach)
+    s.set_vortex([dict(x0=small.x0, y0=small.y0, rstar=workloads.ENSEMBLE_RSTAR, eps=small.eps)], small.mach)
     s.init_vortex(0.0)
     t0 = time.perf_counter()
     s.advance(1, small.dt)
@@ -174,7 +176,7 @@ def cpu_baseline(insts, seconds, nthreads, steps_per_sample=1):
     for inst in sample:
         b = workloads.ensemble_blocks([inst])[0]
         so = orc.System([dict(x=b.x, y=b.y, op_xi=inst.op_id, op_eta=inst.op_id, bc=list(b.bc))], fast=True)
-        so.set_vortex([dict(x0=inst.x0, y0=inst.y0, rstar=0.5, eps=inst.eps)], inst.mach)
+        so.set_vortex([dict(x0=inst.x0, y0=inst.y0, rstar=workloads.ENSEMBLE_RSTAR, eps=inst.eps)], inst.mach)
         so.init_vortex(0.0)
         systems.append(so)
     t0 = time.perf_counter()
@@ -230,23 +232,26 @@ def run_ours(args):
         def barrier():
             pass
 
-    from summationbyparts_b200 import workloads
-    insts = workloads.ensemble_instances(args.ninst, seed=1, first=rank * args.ninst)
+    from summationbyparts_b200 import sharding, workloads
+    first, count = sharding.weak_shard(args.ninst, rank)
+    insts = workloads.ensemble_instances(count, seed=1, first=first)
     points = workloads.ensemble_points(insts)
     stream = torch.cuda.Stream()
     s32 = build_system(insts, "f32c", local)
     s32.set_stream(stream.cuda_stream)
-    tiles = s32.autotune()
+    fixed = tuple(int(v) for v in args.tiles.split(",")) if args.tiles else None
+    if fixed:
+        s32.set_tiles(*fixed)
+        tiles = fixed
+    else:
+        tiles = s32.autotune()
     for _ in range(args.warmup):
         s32.advance(1)
     clocks = Clocks(local)
     clocks.start()
     ms = timed_advance(torch, s32, stream, args.steps, barrier)
     clk = clocks.stop()
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = sharding.max_over_ranks(ms, dist if world > 1 else None)
     total_points = points * world
     value = total_points * args.steps / (ms / 1e3)
     ms_step = ms / args.steps
@@ -255,34 +260,23 @@ def run_ours(args):
     # FP64 plain form on the same ensemble
     fp64 = None
     acc = None
+    s64 = None
     if not args.no_fp64:
         s64 = build_system(insts, "f64", local)
         s64.set_stream(stream.cuda_stream)
-        t64 = s64.autotune()
+        if fixed:
+            s64.set_tiles(*fixed)
+            t64 = fixed
+        else:
+            t64 = s64.autotune()
         for _ in range(args.warmup):
             s64.advance(1)
-        ms64 = timed_advance(torch, s64, stream, args.steps, barrier)
-        t = torch.tensor([ms64], device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms64 = float(t.item())
+        ms64 = sharding.max_over_ranks(timed_advance(torch, s64, stream, args.steps, barrier), dist if world > 1 else None)
         v64 = total_points * args.steps / (ms64 / 1e3)
         fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "tiles": list(t64),
+                "bytes_per_point_update": BYTES_PER_POINT_UPDATE["f64"],
+                "achieved_gbs": BYTES_PER_POINT_UPDATE["f64"] * points / (ms64 / args.steps / 1e3) / 1e9,
                 "speedup_f32_over_f64": value / v64}
-        # same-error check: both forms advanced warmup+steps steps from the same initial data
-        e32, e64 = s32.errors(), s64.errors()
-        import numpy as np
-        rel = np.abs(e32 - e64) / e64
-        n = s32.state_count(0)
-        a = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        b = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        s32.get_state_all(a)
-        s64.get_state_all(b)
-        d = (a - b).norm().item() / b.norm().item()
-        acc = {"steps": args.warmup + args.steps, "l2_err_f64_median": float(np.median(e64)),
-               "l2_err_f32c_median": float(np.median(e32)), "err_rel_diff_max": float(rel.max()),
-               "state_rel_l2_f32c_vs_f64": d}
-        s64.close()
 
     # end to end through the C ABI with host buffers: per step, upload the state from pinned host
     # memory, advance one RK4 step, read the new state back (euler::System::advance_upwind + field())
@@ -308,14 +302,37 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         barrier()
-        me = e0.elapsed_time(e1)
-        t = torch.tensor([me], device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        me = float(t.item())
+        me = sharding.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None)
         e2e = {"value": total_points * ke / (me / 1e3), "unit": UNIT, "h2d_bytes_per_step": n * 8,
                "d2h_bytes_per_step": n * 8, "steps": ke,
                "path": "sbp_system_set_state_all + sbp_system_advance(1) + sbp_system_get_state_all, f64 host state"}
+
+    # same-error check: every instance of both forms to t = 2 (ragged step counts)
+    if s64 is not None and not args.no_accuracy:
+        import numpy as np
+        steps_t2 = [i.steps_to_t2 for i in insts]
+        runs = {}
+        for name, sysx in (("f32c", s32), ("f64", s64)):
+            sysx.init_vortex(0.0)
+            sysx.set_time(0.0)
+            t0 = time.perf_counter()
+            sysx.advance_instances(steps_t2)
+            runs[name] = (sysx.errors(), time.perf_counter() - t0)
+        e32, e64 = runs["f32c"][0], runs["f64"][0]
+        n = s32.state_count(0)
+        a = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        b = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        s32.get_state_all(a)
+        s64.get_state_all(b)
+        rel = np.abs(e32 - e64) / e64
+        acc = {"t_end": 2.0, "instances": len(insts), "point_updates": int(sum(i.side ** 2 * i.steps_to_t2 for i in insts)),
+               "seconds_to_t2_f32c": runs["f32c"][1], "seconds_to_t2_f64": runs["f64"][1],
+               "l2_err_vs_exact_f64_median": float(np.median(e64)), "l2_err_vs_exact_f64_max": float(e64.max()),
+               "l2_err_vs_exact_f32c_median": float(np.median(e32)), "l2_err_vs_exact_f32c_max": float(e32.max()),
+               "err_rel_diff_f32c_vs_f64_max": float(rel.max()),
+               "state_rel_l2_f32c_vs_f64": (a - b).norm().item() / b.norm().item()}
+    if s64 is not None:
+        s64.close()
 
     peak, peak_kind = measured_hbm_peak()
     bpp = BYTES_PER_POINT_UPDATE["f32c"]

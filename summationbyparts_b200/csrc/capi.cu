@@ -1,6 +1,7 @@
 // C ABI: library info, operator tables and the standalone operator / metric entry points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <string>
 
@@ -77,6 +78,67 @@ bool op_info(int op, OpInfo& out) {
 const double* op_h_weights(int op) {
     HostOp o;
     return host_op(op, o) ? o.h : nullptr;
+}
+
+// Stage-kernel coefficient table (layout of coef_base in stage_kernel.cuh): for each operator
+// and kind, [start M rows][end M rows][diagonal], each row `row` elements (zero padded),
+// stride `stride` elements.
+// prec 0 writes doubles; prec 1 writes floats rounded from the f32 literals.
+#define FTAB(TAG)                                                                 \
+    static const float f_##TAG##_DS[] = {SBPC_##TAG##_DIFF_START(SBPC_LIT_F32)};   \
+    static const float f_##TAG##_DD[] = {SBPC_##TAG##_DIFF_DIAG(SBPC_LIT_F32)};
+#define FTAB_DISS(TAG)                                                            \
+    static const float f_##TAG##_SS[] = {SBPC_##TAG##_DISS_START(SBPC_LIT_F32)};   \
+    static const float f_##TAG##_SD[] = {SBPC_##TAG##_DISS_DIAG(SBPC_LIT_F32)};
+FTAB(UPWIND4)
+FTAB(UPWIND4H2)
+FTAB(UPWIND9)
+FTAB(UPWIND9H2)
+FTAB(SBP4)
+FTAB(SBP8)
+FTAB_DISS(UPWIND4)
+FTAB_DISS(UPWIND4H2)
+FTAB_DISS(UPWIND9)
+FTAB_DISS(UPWIND9H2)
+
+template <class T>
+static void fill_one(T* out, const T* st, const T* dg, int M, int N, int D, bool diff, int row) {
+    for (int i = 0; i < M; ++i)
+        for (int k = 0; k < N; ++k) out[i * row + k] = st[i * N + k];
+    for (int i = 0; i < M; ++i)
+        for (int k = 0; k < N; ++k) {
+            const T v = st[(M - 1 - i) * N + (N - 1 - k)];
+            out[(M + i) * row + k] = diff ? -v : v;
+        }
+    for (int d = 0; d < D; ++d) out[2 * M * row + d] = dg[d];
+}
+
+void fill_coef_table(int prec, void* out, int stride, int row) {
+    struct F {
+        const float *ds, *dd, *ss, *sd;
+    };
+    const F ft[6] = {{f_UPWIND4_DS, f_UPWIND4_DD, f_UPWIND4_SS, f_UPWIND4_SD},
+                     {f_UPWIND4H2_DS, f_UPWIND4H2_DD, f_UPWIND4H2_SS, f_UPWIND4H2_SD},
+                     {f_UPWIND9_DS, f_UPWIND9_DD, f_UPWIND9_SS, f_UPWIND9_SD},
+                     {f_UPWIND9H2_DS, f_UPWIND9H2_DD, f_UPWIND9H2_SS, f_UPWIND9H2_SD},
+                     {f_SBP4_DS, f_SBP4_DD, nullptr, nullptr},
+                     {f_SBP8_DS, f_SBP8_DD, nullptr, nullptr}};
+    for (int op = 0; op < 6; ++op) {
+        HostOp o;
+        host_op(op, o);
+        const int M = o.info.M, N = o.info.N, D = o.info.D;
+        for (int kind = 0; kind < 2; ++kind) {
+            const size_t base = (size_t)(2 * op + kind) * stride;
+            if (prec == 0) std::fill((double*)out + base, (double*)out + base + stride, 0.0);
+            else std::fill((float*)out + base, (float*)out + base + stride, 0.0f);
+            if (kind == 1 && !o.info.upwind) continue;
+            if (prec == 0)
+                fill_one<double>((double*)out + base, kind ? o.ss : o.ds, kind ? o.sd : o.dd, M, N, D, kind == 0, row);
+            else
+                fill_one<float>((float*)out + base, kind ? ft[op].ss : ft[op].ds, kind ? ft[op].sd : ft[op].dd, M, N,
+                                D, kind == 0, row);
+        }
+    }
 }
 
 }  // namespace sbp

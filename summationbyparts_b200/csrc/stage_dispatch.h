@@ -2,14 +2,14 @@
 #pragma once
 
 namespace sbp {
-// prec 0 = f64, 1 = f32 compensated.  Returns the kernel entry (a __global__ function pointer
-// usable with cudaLaunchKernel) or nullptr if that operator pair was not built.
-const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw);
+// prec 0 = f64, 1 = f32 compensated; ty = tile rows (16 or 32).  Returns the kernel entry (a
+// __global__ function pointer usable with cudaLaunchKernel) or nullptr if not built.
+const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty);
 
-const void* stage_ptr_f64_u4(int opx, int opy, bool upw);
-const void* stage_ptr_f64_u9(int opx, int opy, bool upw);
-const void* stage_ptr_f64_sbp(int opx, int opy, bool upw);
-const void* stage_ptr_f32_u4(int opx, int opy, bool upw);
-const void* stage_ptr_f32_u9(int opx, int opy, bool upw);
-const void* stage_ptr_f32_sbp(int opx, int opy, bool upw);
+const void* stage_ptr_f64_u4(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f64_u9(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f32_u4(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f32_u9(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty);
 }  // namespace sbp

@@ -4,18 +4,27 @@
 
 namespace sbp {
 
-#define CASE(OX, OY, UPW) \
-    if (opx == OX && opy == OY && upw == UPW) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true>);
+#define CASE(OX, OY, UPW, TYV)                                   \
+    if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
+        return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, TYV>);
 
-const void* stage_ptr_f32_u4(int opx, int opy, bool upw) {
-    CASE(UPWIND4, UPWIND4, true)
-    CASE(UPWIND4, UPWIND4, false)
-    CASE(UPWIND4H2, UPWIND4H2, true)
-    CASE(UPWIND4H2, UPWIND4H2, false)
-    CASE(UPWIND4, UPWIND4H2, true)
-    CASE(UPWIND4, UPWIND4H2, false)
-    CASE(UPWIND4H2, UPWIND4, true)
-    CASE(UPWIND4H2, UPWIND4, false)
+const void* stage_ptr_f32_u4(int opx, int opy, bool upw, int ty) {
+    CASE(UPWIND4, UPWIND4, true, 16)
+    CASE(UPWIND4, UPWIND4, true, 32)
+    CASE(UPWIND4, UPWIND4, false, 16)
+    CASE(UPWIND4, UPWIND4, false, 32)
+    CASE(UPWIND4H2, UPWIND4H2, true, 16)
+    CASE(UPWIND4H2, UPWIND4H2, true, 32)
+    CASE(UPWIND4H2, UPWIND4H2, false, 16)
+    CASE(UPWIND4H2, UPWIND4H2, false, 32)
+    CASE(UPWIND4, UPWIND4H2, true, 16)
+    CASE(UPWIND4, UPWIND4H2, true, 32)
+    CASE(UPWIND4, UPWIND4H2, false, 16)
+    CASE(UPWIND4, UPWIND4H2, false, 32)
+    CASE(UPWIND4H2, UPWIND4, true, 16)
+    CASE(UPWIND4H2, UPWIND4, true, 32)
+    CASE(UPWIND4H2, UPWIND4, false, 16)
+    CASE(UPWIND4H2, UPWIND4, false, 32)
     return nullptr;
 }
 

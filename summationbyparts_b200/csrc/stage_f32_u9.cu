@@ -4,18 +4,27 @@
 
 namespace sbp {
 
-#define CASE(OX, OY, UPW) \
-    if (opx == OX && opy == OY && upw == UPW) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true>);
+#define CASE(OX, OY, UPW, TYV)                                   \
+    if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
+        return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, TYV>);
 
-const void* stage_ptr_f32_u9(int opx, int opy, bool upw) {
-    CASE(UPWIND9, UPWIND9, true)
-    CASE(UPWIND9, UPWIND9, false)
-    CASE(UPWIND9H2, UPWIND9H2, true)
-    CASE(UPWIND9H2, UPWIND9H2, false)
-    CASE(UPWIND9, UPWIND9H2, true)
-    CASE(UPWIND9, UPWIND9H2, false)
-    CASE(UPWIND9H2, UPWIND9, true)
-    CASE(UPWIND9H2, UPWIND9, false)
+const void* stage_ptr_f32_u9(int opx, int opy, bool upw, int ty) {
+    CASE(UPWIND9, UPWIND9, true, 16)
+    CASE(UPWIND9, UPWIND9, true, 32)
+    CASE(UPWIND9, UPWIND9, false, 16)
+    CASE(UPWIND9, UPWIND9, false, 32)
+    CASE(UPWIND9H2, UPWIND9H2, true, 16)
+    CASE(UPWIND9H2, UPWIND9H2, true, 32)
+    CASE(UPWIND9H2, UPWIND9H2, false, 16)
+    CASE(UPWIND9H2, UPWIND9H2, false, 32)
+    CASE(UPWIND9, UPWIND9H2, true, 16)
+    CASE(UPWIND9, UPWIND9H2, true, 32)
+    CASE(UPWIND9, UPWIND9H2, false, 16)
+    CASE(UPWIND9, UPWIND9H2, false, 32)
+    CASE(UPWIND9H2, UPWIND9, true, 16)
+    CASE(UPWIND9H2, UPWIND9, true, 32)
+    CASE(UPWIND9H2, UPWIND9, false, 16)
+    CASE(UPWIND9H2, UPWIND9, false, 32)
     return nullptr;
 }
 

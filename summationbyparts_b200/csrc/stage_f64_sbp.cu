@@ -4,12 +4,15 @@
 
 namespace sbp {
 
-#define CASE(OX, OY, UPW) \
-    if (opx == OX && opy == OY && upw == UPW) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false>);
+#define CASE(OX, OY, UPW, TYV)                                   \
+    if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
+        return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, TYV>);
 
-const void* stage_ptr_f64_sbp(int opx, int opy, bool upw) {
-    CASE(SBP4, SBP4, false)
-    CASE(SBP8, SBP8, false)
+const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty) {
+    CASE(SBP4, SBP4, false, 16)
+    CASE(SBP4, SBP4, false, 32)
+    CASE(SBP8, SBP8, false, 16)
+    CASE(SBP8, SBP8, false, 32)
     return nullptr;
 }
 

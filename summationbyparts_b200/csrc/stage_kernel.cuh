@@ -13,12 +13,15 @@
 // which is the reference's sequence fut = prev; fut += b_j dt k_j (j = 0..3) evaluated
 // incrementally, so the k_j never go to memory.
 //
-// Work decomposition: a persistent grid walks a list of (block, y0, x0) output tiles.  For a
-// tile, phase 1 evaluates the pointwise quantities once per point over the cross-shaped
-// region the stencils read -- Ehat and alpha_u q on the tile rows widened by the xi halo,
-// Fhat and alpha_v q on the tile columns widened by the eta halo (boundary closures widen
-// the halo to the M x N block) -- into shared memory; phase 2 applies the 8 xi and 8 eta
-// stencils from shared memory and finishes each point.
+// Work decomposition.  A persistent grid of 256-thread CTAs walks a list of (block, y0, x0)
+// output tiles of TY rows x 32 columns.  Lane = column, warp w owns rows w*R .. w*R+R-1
+// (R = TY/8).  Phase 1 evaluates the pointwise quantities once per point of the
+// cross-shaped region the stencils read -- Ehat and alpha_u q on the tile rows widened by the
+// xi halo, Fhat and alpha_v q on the tile columns widened by the eta halo (boundary closures
+// widen it to the M x N block) -- into shared memory.  Phase 2 applies the 8 xi and 8 eta
+// stencils from shared memory: the eta sums of a thread's R rows share one register window
+// (R + D - 1 loads for R outputs); interior rows and columns take branch-free paths and only
+// the warps on a block edge run the closure code.
 //
 // Precision: T = double reproduces the reference's f64 arithmetic operation by operation
 // (compile with -fmad=false).  T = float with COMP = true runs fluxes, dissipation and
@@ -26,10 +29,16 @@
 // the SAT terms are computed in f64 from f64 metrics.
 #pragma once
 
+#include <type_traits>
+
 #include "euler_device.cuh"
 #include "sbp_ops.cuh"
 
 namespace sbp {
+
+constexpr int kStageThreads = 256;
+constexpr int kStageWarps = kStageThreads / 32;
+constexpr int kTileX = 32;
 
 template <class T>
 struct StageArgs {
@@ -38,8 +47,6 @@ struct StageArgs {
     const int4* __restrict__ tiles;
     int ntiles;
     int stage;               // 0..3
-    int TY, TX;              // tile shape
-    int WX, HY;              // shared-memory capacities of the xi region width / eta region height
     const T* u_in;           // stage input state, all blocks
     const T* prev_hi;        // state at the start of the step
     const T* prev_lo;        // low part of the state (compensated precision only)
@@ -51,26 +58,429 @@ struct StageArgs {
     const T* met;            // metric planes in T
     const double* met64;     // metric planes in f64 (SAT terms)
     const double* xy;        // coordinates
+    const T* coef;           // operator tables, see coef_base
     double gamma;
     unsigned* status;
 };
 
-template <class T>
-__device__ __forceinline__ T ldg(const T* p) {
-    return __ldg(p);
+// Device coefficient table (one per precision): for operator o and kind k the rows
+// [start block M rows][end block M rows][interior diagonal], each row padded to kCoefRow
+// elements (16-byte aligned rows), at coef_base(o, k).
+constexpr int kCoefRow = 16;
+constexpr int kCoefStride = (2 * 8 + 1) * kCoefRow;
+__host__ __device__ constexpr int coef_base(int op, int kind) { return (2 * op + kind) * kCoefStride; }
+
+// Extent of the input region of a T-long run of outputs: an interior tile reads H beyond each
+// end; a tile that also holds end-closure rows reads from H before its start to the end of
+// the line, at most M - 1 past its own end (tiles start at multiples of T >= M, so only the
+// first tile can hold start-closure rows, and it reads at most max(T + H, N)).
+constexpr int region_extent(int T, int H, int M, int N) {
+    const int a = T + H + (H > M - 1 ? H : M - 1);
+    return a > N ? a : N;
 }
 
-template <int OPX, int OPY, class T, bool UPW, bool COMP>
-__global__ void __launch_bounds__(256) stage_kernel(const StageArgs<T> A) {
+// Block-edge points of one tile get a slot each for their parked k: the first and last block
+// row (32 slots each, by column) and the first and last block column (TY slots each, by row).
+__host__ __device__ constexpr int edge_slots(int TY) { return 2 * kTileX + 2 * TY; }
+__device__ __forceinline__ int edge_slot(int row, int col, int y0, int x0, int nx, int ny, int TY) {
+    if (row == 0) return col - x0;
+    if (row == ny - 1) return kTileX + (col - x0);
+    if (col == 0) return 2 * kTileX + (row - y0);
+    return 2 * kTileX + TY + (row - y0);  // col == nx - 1
+}
+
+// Shared-memory geometry of one tile: xi arrays are TY rows x XP columns, eta arrays HYP rows
+// x 32 columns.
+template <int OPX, int OPY, int TY>
+struct StageGeom {
+    static constexpr int XP = region_extent(kTileX, OpShape<OPX>::H, OpShape<OPX>::M, OpShape<OPX>::N);
+    static constexpr int HYP = region_extent(TY, OpShape<OPY>::H, OpShape<OPY>::M, OpShape<OPY>::N);
+    static constexpr int XA = TY * XP;       // elements of one xi array
+    static constexpr int YA = HYP * kTileX;  // elements of one eta array
+};
+
+template <int OPX, int OPY, int TY, class T>
+constexpr size_t stage_smem(bool upw) {
+    using G = StageGeom<OPX, OPY, TY>;
+    return sizeof(T) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * edge_slots(TY));
+}
+
+// Characteristic SAT of one edge point (euler/src/lib.rs:1150-1252), f64, written row by row
+// so no 4x4 matrix is ever live.  Same operations in the same order as the reference.
+__device__ __forceinline__ void sat_point_rows(double gamma, const double y[4], const double z[4], double hi,
+                                               double sign, double tau, double detj, double detj_d_dx,
+                                               double detj_d_dy, double k[4]) {
+    const double rho = y[0], rhou = y[1], rhov = y[2], e = y[3];
+    const double kx_ = detj_d_dx / detj;
+    const double ky_ = detj_d_dy / detj;
+    const double r = hypot(kx_, ky_);
+    const double kx = kx_ / r, ky = ky_ / r;
+    const double u = rhou / rho, v = rhov / rho;
+    const double theta = kx * u + ky * v;
+    const double p = pressure<double>(gamma, rho, rhou, rhov, e);
+    const double c = sqrt(gamma * p / rho);
+    const double phi2 = (gamma - 1.0) * (u * u + v * v) / 2.0;
+    const double alpha = rho / (1.41421356237309504880 * c);
+    const double phi2_c2 = (phi2 + c * c) / (gamma - 1.0);
+    const double U = kx_ * u + ky_ * v;
+    const double hyp = hypot(kx_, ky_);
+    const double beta = 1.0 / (2.0 * c * c);
+    const double cc = c * c, gm1 = gamma - 1.0;
+    const double r0 = rho - z[0], r1 = rhou - z[1], r2 = rhov - z[2], r3 = e - z[3];
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    t0 += (1.0 - phi2 / cc) * r0;
+    t0 += (gm1 * u / cc) * r1;
+    t0 += (gm1 * v / cc) * r2;
+    t0 += (-gm1 / cc) * r3;
+    t1 += (-(ky * u - kx * v) / rho) * r0;
+    t1 += (ky / rho) * r1;
+    t1 += (-kx / rho) * r2;
+    t1 += 0.0 * r3;
+    t2 += (beta * (phi2 - c * theta)) * r0;
+    t2 += (beta * (kx * c - gm1 * u)) * r1;
+    t2 += (beta * (ky * c - gm1 * v)) * r2;
+    t2 += (beta * gm1) * r3;
+    t3 += (beta * (phi2 + c * theta)) * r0;
+    t3 += (-beta * (kx * c + gm1 * u)) * r1;
+    t3 += (-beta * (ky * c + gm1 * v)) * r2;
+    t3 += (beta * gm1) * r3;
+    const double L0 = U, L2 = U + c * hyp, L3 = U - c * hyp;
+    const double l0 = (L0 + sign * fabs(L0)) * t0;
+    const double l1 = (L0 + sign * fabs(L0)) * t1;
+    const double l2 = (L2 + sign * fabs(L2)) * t2;
+    const double l3 = (L3 + sign * fabs(L3)) * t3;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    s0 += 1.0 * l0;
+    s0 += 0.0 * l1;
+    s0 += alpha * l2;
+    s0 += alpha * l3;
+    s1 += u * l0;
+    s1 += ky * l1;
+    s1 += (alpha * (u + kx * c)) * l2;
+    s1 += (alpha * (u - kx * c)) * l3;
+    s2 += v * l0;
+    s2 += (-kx) * l1;
+    s2 += (alpha * (v + ky * c)) * l2;
+    s2 += (alpha * (v - ky * c)) * l3;
+    s3 += (phi2 / gm1) * l0;
+    s3 += (rho * (ky * u - kx * v)) * l1;
+    s3 += (alpha * (phi2_c2 + c * theta)) * l2;
+    s3 += (alpha * (phi2_c2 - c * theta)) * l3;
+    const double ht = hi * tau;
+    k[0] += ht * s0;
+    k[1] += ht * s1;
+    k[2] += ht * s2;
+    k[3] += ht * s3;
+}
+
+// Pointwise quantities of one point (fluxes, euler/src/lib.rs:680-735; upwind_dissipation
+// 619-674).  Writes the xi-direction values (Ehat, alpha_u q) and/or eta-direction values
+// (Fhat, alpha_v q) into shared memory at the given slots.
+template <class T, bool UPW, bool EXACT>
+__device__ __forceinline__ void pointwise(const T* __restrict__ q, const T* __restrict__ mt, int64_t np, int pt,
+                                          T gamma, T* sxi, int xa, T* seta, int ya, bool want_xi, bool want_eta,
+                                          unsigned& bad) {
+    const T rho = __ldg(q + pt), rhou = __ldg(q + np + pt), rhov = __ldg(q + 2 * np + pt), e = __ldg(q + 3 * np + pt);
+    T E[4], F[4];
+    T p_, u = T(0), v = T(0), c = T(0);
+    if constexpr (EXACT) {
+        // the reference's operations, each division rounded on its own
+        p_ = pressure<T>(gamma, rho, rhou, rhov, e);
+        E[1] = rhou * rhou / rho + p_;
+        E[2] = rhou * rhov / rho;
+        E[3] = rhou * (e + p_) / rho;
+        F[2] = rhov * rhov / rho + p_;
+        F[3] = rhov * (e + p_) / rho;
+        if constexpr (UPW) {
+            u = rhou / rho;
+            v = rhov / rho;
+            c = sqrt(gamma * p_ / rho);
+        }
+    } else {
+        // f32 bulk: one reciprocal of rho shared by every quotient
+        const T ri = T(1) / rho;
+        u = rhou * ri;
+        v = rhov * ri;
+        p_ = (gamma - T(1)) * (e - T(0.5) * (rhou * u + rhov * v));
+        E[1] = rhou * u + p_;
+        E[2] = rhou * v;
+        E[3] = u * (e + p_);
+        F[2] = rhov * v + p_;
+        F[3] = v * (e + p_);
+        if constexpr (UPW) c = sqrt(gamma * p_ * ri);
+    }
+    E[0] = rhou;
+    F[0] = rhov;
+    F[1] = E[2];
+    if constexpr (UPW) {
+        if (!(rho > T(0))) bad |= STATUS_RHO;
+        if (!(p_ > T(0))) bad |= STATUS_P;
+    }
+    if (want_xi) {
+        const T jxx = __ldg(mt + np + pt), jxy = __ldg(mt + 2 * np + pt);
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) sxi[cc * xa] = jxx * E[cc] + jxy * F[cc];
+        if constexpr (UPW) {
+            const T uhat = jxx * u + jxy * v;
+            const T au = fabs(uhat) + c * sqrt(jxx * jxx + jxy * jxy);
+            T* d = sxi + 4 * xa;
+            d[0] = au * rho;
+            d[xa] = au * rhou;
+            d[2 * xa] = au * rhov;
+            d[3 * xa] = au * e;
+        }
+    }
+    if (want_eta) {
+        const T jyx = __ldg(mt + 3 * np + pt), jyy = __ldg(mt + 4 * np + pt);
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) seta[cc * ya] = jyx * E[cc] + jyy * F[cc];
+        if constexpr (UPW) {
+            const T vhat = jyx * u + jyy * v;
+            const T av = fabs(vhat) + c * sqrt(jyx * jyx + jyy * jyy);
+            T* d = seta + 4 * ya;
+            d[0] = av * rho;
+            d[ya] = av * rhou;
+            d[2 * ya] = av * rhov;
+            d[3 * ya] = av * e;
+        }
+    }
+}
+
+// Eta sums of R consecutive rows r0.. of one column from a shared column (stride 32), into
+// out[R], scaled by idx.  `interior` (warp-uniform): every row in [M, ny-M).  EXACT selects the
+// reference's lane split (fma chain for fused columns, unfused sum otherwise); without it the
+// sum is a plain fma chain.  Warps holding closure rows run one N-tap loop per row with the
+// row's coefficients from the table (interior rows predicate off the padding).
+template <int OP, int KIND, class T, int R, bool EXACT>
+__device__ __forceinline__ void eta_rows(const T* __restrict__ col, int ly0, int r0, int nrows, int ny, bool interior,
+                                         bool fused, T idx, const T* __restrict__ ctab, T out[R]) {
+    constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N, D = OpShape<OP>::D, H = OpShape<OP>::H;
+    using C = Coef<OP, KIND, T>;
+    if (interior) {
+        T w[R + D - 1];
+#pragma unroll
+        for (int j = 0; j < R + D - 1; ++j) w[j] = col[(r0 - H + j - ly0) * kTileX];
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            T f = T(0);
+            if (!EXACT || fused) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) f = fma_rn(w[u + d], C::diag(d), f);
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; ++d) f = f + C::diag(d) * w[u + d];
+            }
+            out[u] = f * idx;
+        }
+        return;
+    }
+    const T* tab = ctab + coef_base(OP, KIND);
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        T f = T(0);
+        if (u < nrows) {
+            const int r = r0 + u;
+            const T* crow;
+            int base, ntaps;
+            if (r < M) {
+                crow = tab + r * kCoefRow;
+                base = 0;
+                ntaps = N;
+            } else if (r >= ny - M) {
+                crow = tab + (M + r - (ny - M)) * kCoefRow;
+                base = ny - N;
+                ntaps = N;
+            } else {
+                crow = tab + 2 * M * kCoefRow;
+                base = r - H;
+                ntaps = D;
+            }
+            const T* w = col + (base - ly0) * kTileX;
+            if (!EXACT || fused) {
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                    if (k < ntaps) f = fma_rn(w[k * kTileX], __ldg(crow + k), f);
+            } else {
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                    if (k < ntaps) f = f + __ldg(crow + k) * w[k * kTileX];
+            }
+        }
+        out[u] = f * idx;
+    }
+}
+
+// Xi sums of one kind for the thread's rows: out[c][u] for component c and row ty0 + u of the
+// tile, from the shared xi arrays `sb` (4 component arrays of XA elements, rows of XP, element 0
+// = column lx0).  EXACT: the reference's unfused row order; otherwise an fma chain.  In a tile
+// holding closure columns (`closure_tile`, tile-uniform) every lane loads its own coefficient
+// row once (16-byte vector loads) and runs the same N-tap loop for all 4R sums, so the warp
+// does not diverge; interior lanes predicate off the padding taps.
+template <int OP, int KIND, class T, int R, bool EXACT, int XA, int XP>
+__device__ __forceinline__ void xi_rows(const T* __restrict__ sb, int ty0, int nrows, int lx0, int col, int nx, T idx,
+                                        bool closure_tile, const T* __restrict__ ctab, T out[4][R]) {
+    constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N, D = OpShape<OP>::D, H = OpShape<OP>::H;
+    using C = Coef<OP, KIND, T>;
+    if (!closure_tile) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                T t = T(0);
+                if (u < nrows) {
+                    const T* w = sb + cc * XA + (ty0 + u) * XP + (col - H - lx0);
+                    if constexpr (EXACT) {
+                        t = diag_unfused<OP, KIND, T>([&](int d) { return w[d]; });
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < D; ++d) t = fma_rn(w[d], C::diag(d), t);
+                    }
+                }
+                out[cc][u] = t * idx;
+            }
+        return;
+    }
+    const T* crow;
+    int base, ntaps;
+    {
+        const T* tab = ctab + coef_base(OP, KIND);
+        if (col < M) {
+            crow = tab + col * kCoefRow;
+            base = 0;
+            ntaps = N;
+        } else if (col >= nx - M) {
+            crow = tab + (M + col - (nx - M)) * kCoefRow;
+            base = nx - N;
+            ntaps = N;
+        } else {
+            crow = tab + 2 * M * kCoefRow;
+            base = col - H;
+            ntaps = D;
+        }
+    }
+    constexpr int V = 16 / sizeof(T), NV = (N + V - 1) / V;
+    T cf[NV * V];
+    using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) *reinterpret_cast<VT*>(cf + v * V) = __ldg(reinterpret_cast<const VT*>(crow) + v);
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            T t = T(0);
+            if (u < nrows) {
+                const T* w = sb + cc * XA + (ty0 + u) * XP + (base - lx0);
+                t = cf[0] * w[0];
+#pragma unroll
+                for (int k = 1; k < N; ++k)
+                    if (k < ntaps) {
+                        if constexpr (EXACT) t = t + cf[k] * w[k];
+                        else t = fma_rn(cf[k], w[k], t);
+                    }
+            }
+            out[cc][u] = t * idx;
+        }
+}
+
+// This stage's RK4 update of one component at global element g (see the header comment).
+// `qv` is the stage input at the point (the step-start state in stage 0).
+
+template <class T, bool COMP>
+__device__ __forceinline__ void rk_update(const StageArgs<T>& A, const InstanceDev& I, int64_t g, int64_t np, int cc,
+                                          T qv, T kc) {
+    const int64_t e = g + cc * np;
+    if constexpr (!COMP) {
+        const T cb = T(I.cb[A.stage]);
+        if (A.stage == 0) {
+            A.acc_hi[e] = qv + cb * kc;
+            A.u_out[e] = qv + T(I.ca[0]) * kc;
+        } else if (A.stage < 3) {
+            const T av = A.acc_hi[e];
+            const T pv = __ldg(A.prev_hi + e);
+            A.acc_hi[e] = av + cb * kc;
+            A.u_out[e] = pv + T(I.ca[A.stage]) * kc;
+        } else {
+            A.new_hi[e] = A.acc_hi[e] + cb * kc;
+        }
+    } else {
+        const float cb = float(I.cb[A.stage]);
+        const float kf = float(kc);
+        if (A.stage == 0) {
+            float hi = float(qv);
+            float lo = float(__ldg(A.prev_lo + e));
+            A.u_out[e] = T(hi + float(I.ca[0]) * kf);
+            comp_add(hi, lo, __fmul_rn(cb, kf));
+            A.acc_hi[e] = T(hi);
+            A.acc_lo[e] = T(lo);
+        } else if (A.stage < 3) {
+            float hi = float(A.acc_hi[e]);
+            float lo = float(A.acc_lo[e]);
+            const float pv = float(__ldg(A.prev_hi + e));
+            A.u_out[e] = T(pv + float(I.ca[A.stage]) * kf);
+            comp_add(hi, lo, __fmul_rn(cb, kf));
+            A.acc_hi[e] = T(hi);
+            A.acc_lo[e] = T(lo);
+        } else {
+            float hi = float(A.acc_hi[e]);
+            float lo = float(A.acc_lo[e]);
+            comp_add(hi, lo, __fmul_rn(cb, kf));
+            A.new_hi[e] = T(hi);
+            A.new_lo[e] = T(lo);
+        }
+    }
+}
+
+// SATs of one block-edge point in the reference's order N, S, E, W; k updated in place.
+template <class T>
+__device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int row,
+                                      int col, int pt, const double yv[4], double kv[4]) {
+    const int nx = B.nx, ny = B.ny;
+    const int64_t np = B.npad;
+    const bool on[4] = {row == ny - 1, row == 0, col == nx - 1, col == 0};
+    const double* m64 = A.met64 + B.m_off;
+    const double cst = A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5);
+    const double stime = A.stage == 0 ? I.time : I.time + I.dt * cst;
+    for (int d = 0; d < 4; ++d) {
+        if (!on[d]) continue;
+        double zv[4];
+        const int kind = B.bc_kind[d];
+        if (kind == BC_VORTEX) {
+            const double* xy = A.xy + B.x_off;
+            vortex_point(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+        } else {
+            // This: own opposite edge; Grid(g): neighbour's opposite edge
+            // (boundary_extracts, euler/src/lib.rs:869-930).
+            const BlockDev& Gb = kind == BC_GRID ? A.blocks[B.bc_nb[d]] : B;
+            const T* gq = A.u_in + Gb.q_off;
+            int gp;
+            if (d == NORTH) gp = col;                             // g.south
+            else if (d == SOUTH) gp = (Gb.ny - 1) * Gb.nx + col;  // g.north
+            else if (d == EAST) gp = row * Gb.nx;                 // g.west
+            else gp = row * Gb.nx + (Gb.nx - 1);                  // g.east
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) zv[cc] = double(gq[cc * (int64_t)Gb.npad + gp]);
+        }
+        const bool ns = d == NORTH || d == SOUTH;
+        const double sign = (d == NORTH || d == EAST) ? -1.0 : 1.0;
+        const double tau = (d == NORTH || d == EAST) ? 1.0 : -1.0;
+        const double hi = ns ? B.hi_eta : B.hi_xi;
+        const double ddx = ns ? m64[3 * np + pt] : m64[np + pt];
+        const double ddy = ns ? m64[4 * np + pt] : m64[2 * np + pt];
+        sat_point_rows(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
+    }
+}
+
+template <int OPX, int OPY, class T, bool UPW, bool COMP, int TY>
+__global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs<T> A) {
+    using G = StageGeom<OPX, OPY, TY>;
+    constexpr int R = TY / kStageWarps;
+    constexpr int XA = G::XA, YA = G::YA, XP = G::XP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sm = reinterpret_cast<T*>(smem_raw);
-    const int TY = A.TY, TX = A.TX, WX = A.WX, HY = A.HY;
-    // xi-region arrays: 4 components x TY rows x WX columns; eta-region: 4 x HY x TX.
-    T* sE = sm;
-    T* sDx = sE + 4 * TY * WX;
-    T* sF = UPW ? sDx + 4 * TY * WX : sDx;
-    T* sDy = sF + 4 * HY * TX;
+    T* sE = reinterpret_cast<T*>(smem_raw);       // [UPW ? 8 : 4][TY][XP]: Ehat (0..3), alpha_u q (4..7)
+    T* sF = sE + (UPW ? 8 : 4) * XA;              // [UPW ? 8 : 4][HYP][32]: Fhat (0..3), alpha_v q (4..7)
+    T* sK = sF + (UPW ? 8 : 4) * YA;              // [4][64 + 2 TY]: k of block-edge points awaiting the SAT
     const T gamma = T(A.gamma);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned bad = 0;
 
     for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
@@ -79,7 +489,7 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs<T> A) {
         const int nx = B.nx, ny = B.ny;
         const int64_t np = B.npad;
         const int y0 = td.y, x0 = td.z;
-        const int y1 = min(y0 + TY, ny), x1 = min(x0 + TX, nx);
+        const int y1 = min(y0 + TY, ny), x1 = min(x0 + kTileX, nx);
         const int tw = x1 - x0, th = y1 - y0;
         int lx0, lx1, ly0, ly1;
         region_of<OPX>(x0, x1, nx, lx0, lx1);
@@ -88,234 +498,120 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs<T> A) {
         const T* mt = A.met + B.m_off;
 
         // ---------------- phase 1: pointwise quantities ----------------
+        // One index space over all threads: eta-region points (rows ly0..ly1, 32 slots per row,
+        // slots >= tw idle) followed by the xi-halo points (tile rows x hw columns, packed).
         const int eh = ly1 - ly0;
-        const int hl = x0 - lx0, hr = lx1 - x1, hw = hl + hr;
-        const int nEta = eh * tw, nHalo = th * hw;
-        for (int p = threadIdx.x; p < nEta + nHalo; p += blockDim.x) {
-            int row, col;
-            bool in_eta, in_xi;
-            if (p < nEta) {
-                const int hy = p / tw;
-                row = ly0 + hy;
-                col = x0 + (p - hy * tw);
-                in_eta = true;
-                in_xi = row >= y0 && row < y1;
-            } else {
-                const int qq = p - nEta;
-                const int ty = qq / hw;
-                const int kk = qq - ty * hw;
-                row = y0 + ty;
-                col = kk < hl ? lx0 + kk : x1 + (kk - hl);
-                in_eta = false;
-                in_xi = true;
-            }
-            const int64_t pt = (int64_t)row * nx + col;
-            const T rho = ldg(q + pt), rhou = ldg(q + np + pt), rhov = ldg(q + 2 * np + pt),
-                    e = ldg(q + 3 * np + pt);
-            // fluxes (euler/src/lib.rs:680-735)
-            const T p_ = pressure<T>(gamma, rho, rhou, rhov, e);
-            T E[4], F[4];
-            E[0] = rhou;
-            E[1] = rhou * rhou / rho + p_;
-            E[2] = rhou * rhov / rho;
-            E[3] = rhou * (e + p_) / rho;
-            F[0] = rhov;
-            F[1] = E[2];
-            F[2] = rhov * rhov / rho + p_;
-            F[3] = rhov * (e + p_) / rho;
-            T u = T(0), v = T(0), c = T(0);
-            if constexpr (UPW) {
-                // upwind_dissipation (euler/src/lib.rs:619-674)
-                if (!(rho > T(0))) bad |= STATUS_RHO;
-                if (!(p_ > T(0))) bad |= STATUS_P;
-                u = rhou / rho;
-                v = rhov / rho;
-                c = sqrt(gamma * p_ / rho);
-            }
-            if (in_xi) {
-                const T jxx = ldg(mt + np + pt), jxy = ldg(mt + 2 * np + pt);
-                const int si = (row - y0) * WX + (col - lx0);
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) sE[cc * TY * WX + si] = jxx * E[cc] + jxy * F[cc];
-                if constexpr (UPW) {
-                    const T uhat = jxx * u + jxy * v;
-                    const T au = fabs(uhat) + c * sqrt(jxx * jxx + jxy * jxy);
-                    sDx[si] = au * rho;
-                    sDx[TY * WX + si] = au * rhou;
-                    sDx[2 * TY * WX + si] = au * rhov;
-                    sDx[3 * TY * WX + si] = au * e;
+        const int hl = x0 - lx0, hw = hl + (lx1 - x1);
+        const int n_eta = eh * kTileX, n_all = n_eta + th * hw;
+        const unsigned hw_inv = hw ? (65536u + hw - 1) / hw : 0u;  // exact floor(h / hw) for h < 1024
+        for (int p = threadIdx.x; p < n_all; p += kStageThreads) {
+            if (p < n_eta) {
+                const int row = ly0 + (p >> 5), tx = p & 31;
+                if (tx < tw) {
+                    const int col = x0 + tx;
+                    const bool in_tile = row >= y0 && row < y1;
+                    pointwise<T, UPW, !COMP>(q, mt, np, row * nx + col, gamma,
+                                      in_tile ? sE + (row - y0) * XP + (col - lx0) : nullptr, XA,
+                                      sF + (row - ly0) * kTileX + tx, YA, in_tile, true, bad);
                 }
+            } else {
+                const int h = p - n_eta;
+                const int ty = (int)(((unsigned)h * hw_inv) >> 16);
+                const int hc = h - ty * hw;
+                const int row = y0 + ty;
+                const int col = hc < hl ? lx0 + hc : x1 + (hc - hl);
+                pointwise<T, UPW, !COMP>(q, mt, np, row * nx + col, gamma, sE + ty * XP + (col - lx0), XA, nullptr, YA,
+                                  true, false, bad);
             }
-            if (in_eta) {
-                const T jyx = ldg(mt + 3 * np + pt), jyy = ldg(mt + 4 * np + pt);
-                const int si = (row - ly0) * TX + (col - x0);
+        }
+        __syncthreads();
+
+        // ---------------- phase 2: stencils and stage update ----------------
+        // Interior points finish component by component (k_c, then the RK update of c); points
+        // on a block edge park their k in shared memory for phase 3, where the SAT sees the
+        // full vector.
+        const int r0 = y0 + warp * R;  // first global row of this thread
+        const int nrows = min(R, y1 - r0);
+        const InstanceDev& I = A.inst[B.instance];
+        if (lane < tw && nrows > 0) {
+            const int col = x0 + lane;
+            const T idxx = sizeof(T) == 8 ? T(B.idx_xi) : T(B.idx_xi_f);
+            const T idxy = sizeof(T) == 8 ? T(B.idx_eta) : T(B.idx_eta_f);
+            const bool fused = col < (sizeof(T) == 8 ? B.simd_f64 : B.simd_f32);
+            const bool eta_interior = r0 >= OpShape<OPY>::M && r0 + R <= ny - OpShape<OPY>::M;
+            const bool edge_col = col == 0 || col == nx - 1;
+            const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
+            T detj[R];
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) sF[cc * HY * TX + si] = jyx * E[cc] + jyy * F[cc];
-                if constexpr (UPW) {
-                    const T vhat = jyx * u + jyy * v;
-                    const T av = fabs(vhat) + c * sqrt(jyx * jyx + jyy * jyy);
-                    sDy[si] = av * rho;
-                    sDy[HY * TX + si] = av * rhou;
-                    sDy[2 * HY * TX + si] = av * rhov;
-                    sDy[3 * HY * TX + si] = av * e;
+            for (int u = 0; u < R; ++u) detj[u] = u < nrows ? __ldg(mt + (r0 + u) * nx + col) : T(1);
+            T ex[4][R], dx[4][R];
+            xi_rows<OPX, DIFF, T, R, !COMP, XA, XP>(sE, r0 - y0, nrows, lx0, col, nx, idxx, xi_closure, A.coef, ex);
+            if constexpr (UPW)
+                xi_rows<OPX, DISS, T, R, !COMP, XA, XP>(sE + 4 * XA, r0 - y0, nrows, lx0, col, nx, idxx, xi_closure,
+                                                        A.coef, dx);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                T dF[R];
+                eta_rows<OPY, DIFF, T, R, !COMP>(sF + cc * YA + lane, ly0, r0, nrows, ny, eta_interior, fused, idxy,
+                                                 A.coef, dF);
+                T ay[R];
+                if constexpr (UPW)
+                    eta_rows<OPY, DISS, T, R, !COMP>(sF + (4 + cc) * YA + lane, ly0, r0, nrows, ny, eta_interior,
+                                                     fused, idxy, A.coef, ay);
+#pragma unroll
+                for (int u = 0; u < R; ++u) {
+                    if (u < nrows) {
+                        const int row = r0 + u;
+                        T kc;
+                        if constexpr (UPW) kc = (-ex[cc][u] - dF[u] + dx[cc][u] + ay[u]) / detj[u];
+                        else kc = (-ex[cc][u] - dF[u]) / detj[u];
+                        if (edge_col || row == 0 || row == ny - 1)
+                            sK[cc * edge_slots(TY) + edge_slot(row, col, y0, x0, nx, ny, TY)] = kc;
+                        else
+                            rk_update<T, COMP>(A, I, B.q_off + row * nx + col, np, cc, q[cc * np + row * nx + col],
+                                               kc);
+                    }
                 }
             }
         }
         __syncthreads();
 
-        // ---------------- phase 2: stencils, SAT, stage update ----------------
-        const T idxx = sizeof(T) == 8 ? T(B.idx_xi) : T(B.idx_xi_f);
-        const T idxy = sizeof(T) == 8 ? T(B.idx_eta) : T(B.idx_eta_f);
-        const int simd = sizeof(T) == 8 ? B.simd_f64 : B.simd_f32;
-        const InstanceDev& I = A.inst[B.instance];
-        for (int o = threadIdx.x; o < th * tw; o += blockDim.x) {
-            const int ty = o / tw, tx = o - ty * tw;
-            const int row = y0 + ty, col = x0 + tx;
-            const int64_t pt = (int64_t)row * nx + col;
-            const bool fused = col < simd;
-            const T detj = ldg(mt + pt);
-            T k[4];
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const T* se = sE + cc * TY * WX + ty * WX - lx0;
-                const T* sf = sF + cc * HY * TX + tx - ly0 * TX;
-                const T dE = sum_unfused<OPX, DIFF, T>(col, nx, [&](int kk) { return se[kk]; }) * idxx;
-                const T dF = sum_column<OPY, DIFF, T>(fused, row, ny, [&](int kk) { return sf[kk * TX]; }) * idxy;
-                if constexpr (UPW) {
-                    const T* sdx = sDx + cc * TY * WX + ty * WX - lx0;
-                    const T* sdy = sDy + cc * HY * TX + tx - ly0 * TX;
-                    const T ax = sum_unfused<OPX, DISS, T>(col, nx, [&](int kk) { return sdx[kk]; }) * idxx;
-                    const T ay =
-                        sum_column<OPY, DISS, T>(fused, row, ny, [&](int kk) { return sdy[kk * TX]; }) * idxy;
-                    k[cc] = (-dE - dF + ax + ay) / detj;
-                } else {
-                    k[cc] = (-dE - dF) / detj;
-                }
+        // ---------------- phase 3: SATs of the tile's block-edge points ----------------
+        // One thread per edge slot: first/last block row (by column), first/last block column
+        // (by row, rows 0 and ny-1 excluded: they already own a row slot).
+        {
+            const int s_ = threadIdx.x;
+            int row = -1, col = 0;
+            if (s_ < kTileX) {
+                if (y0 == 0 && s_ < tw) row = 0, col = x0 + s_;
+            } else if (s_ < 2 * kTileX) {
+                if (y1 == ny && s_ - kTileX < tw) row = ny - 1, col = x0 + s_ - kTileX;
+            } else if (s_ < 2 * kTileX + TY) {
+                const int r = y0 + s_ - 2 * kTileX;
+                if (x0 == 0 && r < y1 && r != 0 && r != ny - 1) row = r, col = 0;
+            } else if (s_ < edge_slots(TY)) {
+                const int r = y0 + s_ - 2 * kTileX - TY;
+                if (x1 == nx && r < y1 && r != 0 && r != ny - 1) row = r, col = nx - 1;
             }
-
-            // SATs on block edges, in the reference's order N, S, E, W.
-            const bool on_n = row == ny - 1, on_s = row == 0, on_e = col == nx - 1, on_w = col == 0;
-            if (on_n || on_s || on_e || on_w) {
-                const double* m64 = A.met64 + B.m_off;
+            if (row >= 0) {
+                const int pt = row * nx + col;
                 double yv[4], kv[4];
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc) {
                     yv[cc] = double(q[cc * np + pt]);
-                    kv[cc] = double(k[cc]);
+                    kv[cc] = double(sK[cc * edge_slots(TY) + s_]);
                 }
-                const double C[4] = {0.0, 0.5, 0.5, 1.0};
-                const double stime = A.stage == 0 ? I.time : I.time + I.dt * C[A.stage];
+                sat_edge<T>(A, I, B, row, col, pt, yv, kv);
 #pragma unroll
-                for (int d = 0; d < 4; ++d) {
-                    const bool on = d == NORTH ? on_n : d == SOUTH ? on_s : d == EAST ? on_e : on_w;
-                    if (!on) continue;
-                    double zv[4];
-                    const int kind = B.bc_kind[d];
-                    if (kind == BC_VORTEX) {
-                        const double* xy = A.xy + B.x_off;
-                        vortex_point(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
-                    } else {
-                        // This: own opposite edge; Grid(g): neighbour's opposite edge
-                        // (boundary_extracts, euler/src/lib.rs:869-930).
-                        const BlockDev& G = kind == BC_GRID ? A.blocks[B.bc_nb[d]] : B;
-                        const T* gq = A.u_in + G.q_off;
-                        int64_t gp;
-                        if (d == NORTH) gp = col;                                          // g.south
-                        else if (d == SOUTH) gp = (int64_t)(G.ny - 1) * G.nx + col;        // g.north
-                        else if (d == EAST) gp = (int64_t)row * G.nx;                      // g.west
-                        else gp = (int64_t)row * G.nx + (G.nx - 1);                        // g.east
-#pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) zv[cc] = double(gq[cc * (int64_t)G.npad + gp]);
-                    }
-                    const bool ns = d == NORTH || d == SOUTH;
-                    const double sign = (d == NORTH || d == EAST) ? -1.0 : 1.0;
-                    const double tau = (d == NORTH || d == EAST) ? 1.0 : -1.0;
-                    const double hi = ns ? B.hi_eta : B.hi_xi;
-                    const double ddx = ns ? m64[3 * np + pt] : m64[np + pt];
-                    const double ddy = ns ? m64[4 * np + pt] : m64[2 * np + pt];
-                    sat_point(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
-                }
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) k[cc] = T(kv[cc]);
-            }
-
-            // RK4 stage update
-            const int64_t g = B.q_off + pt;
-            if (!COMP) {
-                const T cb = T(I.cb[A.stage]);
-                if (A.stage == 0) {
-                    const T ca = T(I.ca[0]);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const T pv = q[cc * np + pt];
-                        A.acc_hi[g + cc * np] = pv + cb * k[cc];
-                        A.u_out[g + cc * np] = pv + ca * k[cc];
-                    }
-                } else if (A.stage < 3) {
-                    const T ca = T(I.ca[A.stage]);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const T av = A.acc_hi[g + cc * np];
-                        const T pv = ldg(A.prev_hi + g + cc * np);
-                        A.acc_hi[g + cc * np] = av + cb * k[cc];
-                        A.u_out[g + cc * np] = pv + ca * k[cc];
-                    }
-                } else {
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const T av = A.acc_hi[g + cc * np];
-                        A.new_hi[g + cc * np] = av + cb * k[cc];
-                    }
-                }
-            } else {
-                const float cb = float(I.cb[A.stage]);
-                if (A.stage == 0) {
-                    const float ca = float(I.ca[0]);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        float hi = float(q[cc * np + pt]);
-                        float lo = float(ldg(A.prev_lo + g + cc * np));
-                        const float kk = float(k[cc]);
-                        A.u_out[g + cc * np] = T(hi + ca * kk);
-                        comp_add(hi, lo, __fmul_rn(cb, kk));
-                        A.acc_hi[g + cc * np] = T(hi);
-                        A.acc_lo[g + cc * np] = T(lo);
-                    }
-                } else if (A.stage < 3) {
-                    const float ca = float(I.ca[A.stage]);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        float hi = float(A.acc_hi[g + cc * np]);
-                        float lo = float(A.acc_lo[g + cc * np]);
-                        const float kk = float(k[cc]);
-                        const float pv = float(ldg(A.prev_hi + g + cc * np));
-                        A.u_out[g + cc * np] = T(pv + ca * kk);
-                        comp_add(hi, lo, __fmul_rn(cb, kk));
-                        A.acc_hi[g + cc * np] = T(hi);
-                        A.acc_lo[g + cc * np] = T(lo);
-                    }
-                } else {
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        float hi = float(A.acc_hi[g + cc * np]);
-                        float lo = float(A.acc_lo[g + cc * np]);
-                        comp_add(hi, lo, __fmul_rn(cb, float(k[cc])));
-                        A.new_hi[g + cc * np] = T(hi);
-                        A.new_lo[g + cc * np] = T(lo);
-                    }
-                }
+                for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, I, B.q_off + pt, np, cc, T(yv[cc]), T(kv[cc]));
             }
         }
-        __syncthreads();
+        // No barrier here: phase 3 reads only sK and global memory, and the next tile's phase 1
+        // writes only the xi/eta arrays (whose readers all passed the barrier after phase 2);
+        // sK is rewritten only in the next tile's phase 2, behind the next barrier.  The edge
+        // threads' SAT work overlaps the other threads' next phase 1.
     }
     if (bad) atomicOr(A.status, bad);
-}
-
-// Shared memory bytes of one CTA.
-template <class T>
-inline size_t stage_smem_bytes(bool upw, int TY, int TX, int WX, int HY) {
-    const size_t per = (size_t)4 * TY * WX + (size_t)4 * HY * TX;
-    return sizeof(T) * per * (upw ? 2 : 1);
 }
 
 }  // namespace sbp

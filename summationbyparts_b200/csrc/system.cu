@@ -24,13 +24,14 @@
 
 namespace sbp {
 const double* op_h_weights(int op);
+void fill_coef_table(int prec, void* out, int stride, int row);
 
-const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw) {
-    using F = const void* (*)(int, int, bool);
+const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty) {
+    using F = const void* (*)(int, int, bool, int);
     static const F f64[] = {stage_ptr_f64_u4, stage_ptr_f64_u9, stage_ptr_f64_sbp};
     static const F f32[] = {stage_ptr_f32_u4, stage_ptr_f32_u9, stage_ptr_f32_sbp};
     for (F f : (prec == 0 ? f64 : f32)) {
-        const void* p = f(opx, opy, upw);
+        const void* p = f(opx, opy, upw, ty);
         if (p) return p;
     }
     return nullptr;
@@ -50,6 +51,17 @@ void region_host(int op, int a0, int a1, int n, int& lo, int& hi) {
 }
 
 int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
+
+// Shared memory of one stage-kernel CTA (mirrors StageGeom in stage_kernel.cuh).
+size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
+    OpInfo ox, oy;
+    op_info(opx, ox);
+    op_info(opy, oy);
+    const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
+    const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
+    const size_t elems = (size_t)(4 * ty * xp + 4 * hyp * kTileX) * (upw ? 2 : 1) + 4 * edge_slots(ty);
+    return elems * (prec == 0 ? sizeof(double) : sizeof(float));
+}
 
 struct Group {
     int opx, opy;
@@ -98,8 +110,9 @@ struct sbp_system {
     unsigned* status = nullptr;
     double* d_sums = nullptr;
     unsigned long long* d_speeds = nullptr;
+    void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
     // schedule
-    int TY = 32, TX = 32, threads = 256;
+    int TY = 16, TX = kTileX, threads = kStageThreads;
     std::vector<int> active;
     std::vector<Group> groups;
     bool sched_dirty = true;
@@ -134,7 +147,8 @@ void destroy_all(sbp_system* s) {
     free_groups(s);
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
-                    s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds};
+                    s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
+                    s->d_coef};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -181,10 +195,6 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.tiles = g.d_tiles;
     a.ntiles = g.ntiles;
     a.stage = stage;
-    a.TY = s->TY;
-    a.TX = s->TX;
-    a.WX = g.WX;
-    a.HY = g.HY;
     T* prev = static_cast<T*>(s->prev_hi);
     T* uA = static_cast<T*>(s->uA);
     T* uB = static_cast<T*>(s->uB);
@@ -201,6 +211,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.met = s->prec == 0 ? reinterpret_cast<const T*>(s->met64) : reinterpret_cast<const T*>(s->met32);
     a.met64 = s->met64;
     a.xy = s->xy;
+    a.coef = static_cast<const T*>(s->d_coef);
     a.gamma = s->gamma;
     a.status = s->status;
     return a;
@@ -240,7 +251,7 @@ sbp_status build_schedule(sbp_system* s) {
             g.opx = B.op_xi;
             g.opy = B.op_eta;
             g.upw = upw;
-            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw);
+            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw, TY);
             if (!g.fn) {
                 set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", B.op_xi, B.op_eta);
                 return SBP_ERR_UNSUPPORTED;
@@ -274,8 +285,18 @@ sbp_status build_schedule(sbp_system* s) {
     for (size_t gi = 0; gi < s->groups.size(); ++gi) {
         Group& g = s->groups[gi];
         g.ntiles = (int)tiles[gi].size();
-        g.smem = s->prec == 0 ? stage_smem_bytes<double>(g.upw, TY, TX, g.WX, g.HY)
-                              : stage_smem_bytes<float>(g.upw, TY, TX, g.WX, g.HY);
+        g.smem = stage_smem_host(s->prec, g.opx, g.opy, g.upw, TY);
+        {
+            OpInfo ox, oy;
+            op_info(g.opx, ox);
+            op_info(g.opy, oy);
+            // every region fits the kernel's fixed shared-memory geometry
+            if (g.WX > region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N) ||
+                g.HY > region_extent(TY, (oy.D - 1) / 2, oy.M, oy.N)) {
+                set_error("internal: tile region exceeds the shared-memory geometry");
+                return SBP_ERR_INVALID_ARGUMENT;
+            }
+        }
         if (g.smem > s->smem_optin) {
             set_error("tile %dx%d needs %zu bytes of shared memory (limit %zu)", TY, TX, g.smem, s->smem_optin);
             return SBP_ERR_INVALID_ARGUMENT;
@@ -530,6 +551,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->status, sizeof(unsigned));
     e = e ?: alloc((void**)&s->d_sums, nblocks * sizeof(double));
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
+    e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
     cudaStream_t st = s->stream;
     e = e ?: cudaMemsetAsync(s->prev_hi, 0, s->nq * ts, st);
@@ -544,6 +566,9 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: cudaMemcpyAsync(s->d_blocks, s->hb.data(), nblocks * sizeof(BlockDev), cudaMemcpyHostToDevice, st);
     e = e ?: cudaMemcpyAsync(s->d_inst, s->hi.data(), ninstances * sizeof(InstanceDev), cudaMemcpyHostToDevice, st);
     e = e ?: cudaMemcpyAsync(s->d_hoff, s->hoff.data(), nblocks * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    std::vector<double> coef_host(12 * kCoefStride);  // large enough for either precision
+    fill_coef_table(s->prec, coef_host.data(), kCoefStride, kCoefRow);
+    e = e ?: cudaMemcpyAsync(s->d_coef, coef_host.data(), 12 * kCoefStride * ts, cudaMemcpyHostToDevice, st);
     {
         std::vector<int64_t> p8(nblocks);
         for (int b = 0; b < nblocks; ++b) p8[b] = 2 * s->dense_off[b];
@@ -606,7 +631,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         OpInfo ox, oy;
         op_info(s->hb[b].op_xi, ox);
         op_info(s->hb[b].op_eta, oy);
-        if (!stage_kernel_ptr(s->prec, s->hb[b].op_xi, s->hb[b].op_eta, ox.upwind && oy.upwind)) {
+        if (!stage_kernel_ptr(s->prec, s->hb[b].op_xi, s->hb[b].op_eta, ox.upwind && oy.upwind, 16)) {
             set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", s->hb[b].op_xi,
                       s->hb[b].op_eta);
             return fail(SBP_ERR_UNSUPPORTED);
@@ -894,17 +919,14 @@ sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double
 
 sbp_status sbp_system_set_tiles(sbp_system* sys, int ty, int tx, int threads) {
     clear_error();
-    if (!sys || ty < 8 || tx < 8 || ty > 256 || tx > 256) {
-        set_error("tile dimensions must be within [8, 256]");
-        return SBP_ERR_INVALID_ARGUMENT;
-    }
-    if (threads != 0 && (threads % 32 != 0 || threads > 256 || threads < 32)) {
-        set_error("threads must be a multiple of 32 in [32, 256]");
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    if ((ty != 16 && ty != 32) || tx != kTileX || (threads != 0 && threads != kStageThreads)) {
+        set_error("tiles are 16 or 32 rows x %d columns with %d threads", kTileX, kStageThreads);
         return SBP_ERR_INVALID_ARGUMENT;
     }
     sys->TY = ty;
     sys->TX = tx;
-    if (threads) sys->threads = threads;
+    sys->threads = kStageThreads;
     sys->sched_dirty = true;
     return SBP_OK;
 }
@@ -919,8 +941,7 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads) 
             return SBP_ERR_INVALID_ARGUMENT;
         }
     std::fill(sys->active.begin(), sys->active.end(), 1);
-    static const int cand[][3] = {{16, 32, 256}, {32, 32, 256}, {16, 64, 256}, {32, 64, 256},
-                                  {8, 64, 256},  {64, 32, 256}, {8, 32, 128},  {16, 16, 128}};
+    static const int cand[][3] = {{16, kTileX, kStageThreads}, {32, kTileX, kStageThreads}};
     const size_t ts = sys->tsize();
     // save state and times
     void* save_hi = nullptr;

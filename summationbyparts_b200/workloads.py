@@ -119,6 +119,14 @@ def multiblock_dt(blocks) -> float:
 
 
 # ----- configuration 3: batched ensemble ----------------------------------------------------
+# Vortex radius of the ensemble: the reference's own System::init_with_vortex radius
+# (euler/src/lib.rs:83-103).  With rstar = 0.5 the strongest draws (eps ~ 1.4, Mach ~ 0.7) are
+# under-resolved on the coarsest grids and lose positivity before t = 2 under the reference's
+# scheme itself (5 of the 125 draws with side <= 100, Upwind4), where the reference would stop
+# on assert!(p > 0.0) (euler/src/lib.rs:642).
+ENSEMBLE_RSTAR = 1.0
+
+
 @dataclass
 class Instance:
     x0: float
@@ -138,7 +146,7 @@ class Instance:
 
     @property
     def vortex(self) -> VortexParameters:
-        return VortexParameters([Vortice(self.x0, self.y0, 0.5, self.eps)], mach=self.mach)
+        return VortexParameters([Vortice(self.x0, self.y0, ENSEMBLE_RSTAR, self.eps)], mach=self.mach)
 
 
 def ensemble_instances(n: int = 512, seed: int = 1, first: int = 0) -> list[Instance]:

