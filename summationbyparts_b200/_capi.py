@@ -1,8 +1,8 @@
 """ctypes binding of libsbp_b200.so (the C ABI declared in include/sbp_b200.h).
 
-The library is loaded from summationbyparts_b200/_lib/.  There is no fallback: if the
-shared library is missing or fails to load, importing this module raises, so a run can
-never silently compute on the CPU.
+The library is loaded from summationbyparts_b200/_lib/ on first use (so the package can be
+imported to build it).  There is no fallback: if the shared library is missing or fails to
+load, the first call raises, so a run can never silently compute on the CPU.
 """
 from __future__ import annotations
 
@@ -57,6 +57,7 @@ SIGNATURES = {
     "sbp_dissxi": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "sbp_disseta": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "sbp_metrics": (_i, [_i, _i, _vp, _vp, _i64, _i64, _vp, _vp]),
+    "sbp_metrics_noalloc": (_i, [_i, _i, _vp, _vp, _i64, _i64, _vp, _vp]),
     "sbp_system_create": (_i, [_i, ctypes.POINTER(BlockDesc), _i, _i, _i, _d, ctypes.POINTER(_vp)]),
     "sbp_system_destroy": (_i, [_vp]),
     "sbp_system_set_force_trad": (_i, [_vp, _i]),
@@ -95,7 +96,18 @@ def _load() -> ctypes.CDLL:
     return lib
 
 
-lib = _load()
+class _Library:
+    """Loads libsbp_b200.so on first attribute access."""
+
+    _handle = None
+
+    def __getattr__(self, name):
+        if _Library._handle is None:
+            _Library._handle = _load()
+        return getattr(_Library._handle, name)
+
+
+lib = _Library()
 
 
 def check(status: int) -> None:
