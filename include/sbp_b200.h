@@ -128,6 +128,19 @@ sbp_status sbp_disseta(int op, int dtype, const void* d_prev, void* d_fut, int64
 sbp_status sbp_metrics(int op_xi, int op_eta, const double* d_x, const double* d_y, int64_t ny, int64_t nx,
                        double* d_metrics, void* stream);
 
+/* Grid metrics like sbp_metrics, with no device allocation.  This entry point has no
+ * counterpart in the reference.  It serves callers that cannot allocate device memory where
+ * they need metrics (all device memory belongs to another runtime's pool or arena, or a
+ * time-critical loop forbids allocator calls, which can synchronise the device): its working
+ * memory is a fixed array inside the library (8 MiB + 256 B on every GPU that loads it, kept
+ * until exit) instead of cudaMallocAsync.
+ * Limits: at most 512 x 512 = 262144 points per call (larger grids return SBP_ERR_SHAPE);
+ * calls share the array, so calls whose GPU work overlaps race and must not be issued; the
+ * first call on each device looks the array up with cudaGetSymbolAddress and should come
+ * before any stream capture.  Synchronises `stream` to read the Jacobian check. */
+sbp_status sbp_metrics_noalloc(int op_xi, int op_eta, const double* d_x, const double* d_y, int64_t ny,
+                               int64_t nx, double* d_metrics, void* stream);
+
 /* ---- systems: euler::System, multigrid::System, ensembles --------------- */
 
 /* Build a system on `device`: copies the grids in, builds the f64 metrics on the device

@@ -33,6 +33,7 @@ UNITS = {
     "system.cu": EXACT,
     "system_kernels.cu": EXACT,
     "op_apply.cu": EXACT,
+    "metrics_noalloc.cu": EXACT,
     "stage_f64_u4.cu": EXACT,
     "stage_f64_u9.cu": EXACT,
     "stage_f64_sbp.cu": EXACT,
