@@ -99,10 +99,15 @@ struct StageGeom {
     static constexpr int YA = HYP * kTileX;  // elements of one eta array
 };
 
+// Phase-2 operands staged in shared memory by cp.async while phase 1 runs (compensated-f32
+// kernel): slot 0 detJ, then up to three state arrays x 4 components (see stage_operands).
+constexpr int kStageSlots = 13;
+__host__ __device__ constexpr int staged_elems(bool comp, int TY) { return comp ? kStageSlots * TY * kTileX : 0; }
+
 template <int OPX, int OPY, int TY, class T>
-constexpr size_t stage_smem(bool upw) {
+constexpr size_t stage_smem(bool upw, bool comp) {
     using G = StageGeom<OPX, OPY, TY>;
-    return sizeof(T) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * edge_slots(TY));
+    return sizeof(T) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * edge_slots(TY) + staged_elems(comp, TY));
 }
 
 // Characteristic SAT of one edge point (euler/src/lib.rs:1150-1252), f64, written row by row
@@ -382,6 +387,61 @@ __device__ __forceinline__ void xi_rows(const T* __restrict__ sb, int ty0, int n
         }
 }
 
+// Asynchronous global -> shared copy of one element (cp.async, sm_80+), and the wait for all
+// of this thread's copies.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem));
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The state arrays this stage's RK update reads (compensated form), in slot order:
+// stage 0: prev_lo; stages 1, 2: acc_hi, acc_lo, prev_hi; stage 3: acc_hi, acc_lo.
+template <class T>
+__device__ __forceinline__ int stage_operands(const StageArgs<T>& A, const T* src[3]) {
+    if (A.stage == 0) {
+        src[0] = A.prev_lo;
+        return 1;
+    }
+    src[0] = A.acc_hi;
+    src[1] = A.acc_lo;
+    src[2] = A.prev_hi;
+    return A.stage < 3 ? 3 : 2;
+}
+
+// Compensated RK update of one component with its operands taken from the staging slots
+// (sop(a) = operand array a of this component at this point); same arithmetic as rk_update.
+template <class T, class SOP>
+__device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, const InstanceDev& I, int64_t e, T qv, T kc,
+                                                 SOP sop) {
+    const float cb = float(I.cb[A.stage]);
+    const float kf = float(kc);
+    if (A.stage == 0) {
+        float hi = float(qv);
+        float lo = float(sop(0));
+        A.u_out[e] = T(hi + float(I.ca[0]) * kf);
+        comp_add(hi, lo, __fmul_rn(cb, kf));
+        A.acc_hi[e] = T(hi);
+        A.acc_lo[e] = T(lo);
+    } else if (A.stage < 3) {
+        float hi = float(sop(0));
+        float lo = float(sop(1));
+        const float pv = float(sop(2));
+        A.u_out[e] = T(pv + float(I.ca[A.stage]) * kf);
+        comp_add(hi, lo, __fmul_rn(cb, kf));
+        A.acc_hi[e] = T(hi);
+        A.acc_lo[e] = T(lo);
+    } else {
+        float hi = float(sop(0));
+        float lo = float(sop(1));
+        comp_add(hi, lo, __fmul_rn(cb, kf));
+        A.new_hi[e] = T(hi);
+        A.new_lo[e] = T(lo);
+    }
+}
+
 // This stage's RK4 update of one component at global element g (see the header comment).
 // `qv` is the stage input at the point (the step-start state in stage 0).
 
@@ -479,6 +539,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
     T* sE = reinterpret_cast<T*>(smem_raw);       // [UPW ? 8 : 4][TY][XP]: Ehat (0..3), alpha_u q (4..7)
     T* sF = sE + (UPW ? 8 : 4) * XA;              // [UPW ? 8 : 4][HYP][32]: Fhat (0..3), alpha_v q (4..7)
     T* sK = sF + (UPW ? 8 : 4) * YA;              // [4][64 + 2 TY]: k of block-edge points awaiting the SAT
+    T* sR = sK + 4 * edge_slots(TY);              // [13][TY][32]: staged phase-2 operands (COMP)
     const T gamma = T(A.gamma);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned bad = 0;
@@ -498,6 +559,28 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         const T* mt = A.met + B.m_off;
 
         // ---------------- phase 1: pointwise quantities ----------------
+        // Stage this thread's phase-2 operands (detJ, RK state) into shared memory; the copies
+        // run while phase 1 computes.
+        if constexpr (COMP) {
+            const int pr0 = y0 + warp * R, prn = min(R, y1 - pr0);
+            if (lane < tw) {
+                const T* src[3];
+                const int nsrc = stage_operands<T>(A, src);
+#pragma unroll
+                for (int u = 0; u < R; ++u)
+                    if (u < prn) {
+                        const int ty = pr0 - y0 + u;
+                        const int pt = (pr0 + u) * nx + x0 + lane;
+                        T* slot = sR + ty * kTileX + lane;
+                        cp_async_elem(slot, mt + pt);
+                        for (int a = 0; a < nsrc; ++a)
+#pragma unroll
+                            for (int cc = 0; cc < 4; ++cc)
+                                cp_async_elem(slot + (1 + 4 * a + cc) * TY * kTileX, src[a] + B.q_off + cc * np + pt);
+                    }
+            }
+        }
+
         // One index space over all threads: eta-region points (rows ly0..ly1, 32 slots per row,
         // slots >= tw idle) followed by the xi-halo points (tile rows x hw columns, packed).
         const int eh = ly1 - ly0;
@@ -524,6 +607,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                                   true, false, bad);
             }
         }
+        if constexpr (COMP) cp_async_wait_all();
         __syncthreads();
 
         // ---------------- phase 2: stencils and stage update ----------------
@@ -543,7 +627,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
             const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
             T detj[R];
 #pragma unroll
-            for (int u = 0; u < R; ++u) detj[u] = u < nrows ? __ldg(mt + (r0 + u) * nx + col) : T(1);
+            for (int u = 0; u < R; ++u) {
+                if constexpr (COMP) detj[u] = u < nrows ? sR[(r0 - y0 + u) * kTileX + lane] : T(1);
+                else detj[u] = u < nrows ? __ldg(mt + (r0 + u) * nx + col) : T(1);
+            }
             T ex[4][R], dx[4][R];
             xi_rows<OPX, DIFF, T, R, !COMP, XA, XP>(sE, r0 - y0, nrows, lx0, col, nx, idxx, xi_closure, A.coef, ex);
             if constexpr (UPW)
@@ -567,6 +654,9 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                         else kc = (-ex[cc][u] - dF[u]) / detj[u];
                         if (edge_col || row == 0 || row == ny - 1)
                             sK[cc * edge_slots(TY) + edge_slot(row, col, y0, x0, nx, ny, TY)] = kc;
+                        else if constexpr (COMP)
+                            rk_update_staged<T>(A, I, B.q_off + row * nx + col + cc * np, q[cc * np + row * nx + col], kc,
+                                                [&](int a) { return sR[((1 + 4 * a + cc) * TY + row - y0) * kTileX + lane]; });
                         else
                             rk_update<T, COMP>(A, I, B.q_off + row * nx + col, np, cc, q[cc * np + row * nx + col],
                                                kc);

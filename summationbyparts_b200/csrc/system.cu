@@ -59,7 +59,8 @@ size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
     op_info(opy, oy);
     const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
     const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
-    const size_t elems = (size_t)(4 * ty * xp + 4 * hyp * kTileX) * (upw ? 2 : 1) + 4 * edge_slots(ty);
+    const size_t elems =
+        (size_t)(4 * ty * xp + 4 * hyp * kTileX) * (upw ? 2 : 1) + 4 * edge_slots(ty) + staged_elems(prec == 1, ty);
     return elems * (prec == 0 ? sizeof(double) : sizeof(float));
 }
 
