@@ -398,12 +398,13 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // The state arrays this stage's RK update reads (compensated form), in slot order:
-// stage 0: prev_lo; stages 1, 2: acc_hi, acc_lo, prev_hi; stage 3: acc_hi, acc_lo.
+// stage 0: prev_lo, u_in (= prev_hi); stages 1, 2: acc_hi, acc_lo, prev_hi; stage 3: acc_hi, acc_lo.
 template <class T>
 __device__ __forceinline__ int stage_operands(const StageArgs<T>& A, const T* src[3]) {
     if (A.stage == 0) {
         src[0] = A.prev_lo;
-        return 1;
+        src[1] = A.u_in;
+        return 2;
     }
     src[0] = A.acc_hi;
     src[1] = A.acc_lo;
@@ -411,17 +412,16 @@ __device__ __forceinline__ int stage_operands(const StageArgs<T>& A, const T* sr
     return A.stage < 3 ? 3 : 2;
 }
 
-// Compensated RK update of one component with its operands taken from the staging slots
-// (sop(a) = operand array a of this component at this point); same arithmetic as rk_update.
+// Compensated RK update of one component at element e with its operands taken from the
+// staging slots (sop(a) = operand array a of this component at this point); same arithmetic
+// as rk_update.  cb, ca: this stage's B and A tableau entries times dt, already in f32.
 template <class T, class SOP>
-__device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, const InstanceDev& I, int64_t e, T qv, T kc,
-                                                 SOP sop) {
-    const float cb = float(I.cb[A.stage]);
+__device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, int64_t e, float cb, float ca, T kc, SOP sop) {
     const float kf = float(kc);
     if (A.stage == 0) {
-        float hi = float(qv);
+        float hi = float(sop(1));
         float lo = float(sop(0));
-        A.u_out[e] = T(hi + float(I.ca[0]) * kf);
+        A.u_out[e] = T(hi + ca * kf);
         comp_add(hi, lo, __fmul_rn(cb, kf));
         A.acc_hi[e] = T(hi);
         A.acc_lo[e] = T(lo);
@@ -429,7 +429,7 @@ __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, const In
         float hi = float(sop(0));
         float lo = float(sop(1));
         const float pv = float(sop(2));
-        A.u_out[e] = T(pv + float(I.ca[A.stage]) * kf);
+        A.u_out[e] = T(pv + ca * kf);
         comp_add(hi, lo, __fmul_rn(cb, kf));
         A.acc_hi[e] = T(hi);
         A.acc_lo[e] = T(lo);
@@ -442,48 +442,46 @@ __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, const In
     }
 }
 
-// This stage's RK4 update of one component at global element g (see the header comment).
-// `qv` is the stage input at the point (the step-start state in stage 0).
-
+// This stage's RK4 update of one component at element e (see the header comment), operands
+// read from global memory.  `qv` is the stage input at the point (the step-start state in
+// stage 0); cb, ca: this stage's B and A tableau entries times dt (ca unused in stage 3).
 template <class T, bool COMP>
-__device__ __forceinline__ void rk_update(const StageArgs<T>& A, const InstanceDev& I, int64_t g, int64_t np, int cc,
-                                          T qv, T kc) {
-    const int64_t e = g + cc * np;
+__device__ __forceinline__ void rk_update(const StageArgs<T>& A, int64_t e, T qv, T kc, double cb, double ca) {
     if constexpr (!COMP) {
-        const T cb = T(I.cb[A.stage]);
+        const T cbt = T(cb);
         if (A.stage == 0) {
-            A.acc_hi[e] = qv + cb * kc;
-            A.u_out[e] = qv + T(I.ca[0]) * kc;
+            A.acc_hi[e] = qv + cbt * kc;
+            A.u_out[e] = qv + T(ca) * kc;
         } else if (A.stage < 3) {
             const T av = A.acc_hi[e];
             const T pv = __ldg(A.prev_hi + e);
-            A.acc_hi[e] = av + cb * kc;
-            A.u_out[e] = pv + T(I.ca[A.stage]) * kc;
+            A.acc_hi[e] = av + cbt * kc;
+            A.u_out[e] = pv + T(ca) * kc;
         } else {
-            A.new_hi[e] = A.acc_hi[e] + cb * kc;
+            A.new_hi[e] = A.acc_hi[e] + cbt * kc;
         }
     } else {
-        const float cb = float(I.cb[A.stage]);
+        const float cbf = float(cb);
         const float kf = float(kc);
         if (A.stage == 0) {
             float hi = float(qv);
             float lo = float(__ldg(A.prev_lo + e));
-            A.u_out[e] = T(hi + float(I.ca[0]) * kf);
-            comp_add(hi, lo, __fmul_rn(cb, kf));
+            A.u_out[e] = T(hi + float(ca) * kf);
+            comp_add(hi, lo, __fmul_rn(cbf, kf));
             A.acc_hi[e] = T(hi);
             A.acc_lo[e] = T(lo);
         } else if (A.stage < 3) {
             float hi = float(A.acc_hi[e]);
             float lo = float(A.acc_lo[e]);
             const float pv = float(__ldg(A.prev_hi + e));
-            A.u_out[e] = T(pv + float(I.ca[A.stage]) * kf);
-            comp_add(hi, lo, __fmul_rn(cb, kf));
+            A.u_out[e] = T(pv + float(ca) * kf);
+            comp_add(hi, lo, __fmul_rn(cbf, kf));
             A.acc_hi[e] = T(hi);
             A.acc_lo[e] = T(lo);
         } else {
             float hi = float(A.acc_hi[e]);
             float lo = float(A.acc_lo[e]);
-            comp_add(hi, lo, __fmul_rn(cb, kf));
+            comp_add(hi, lo, __fmul_rn(cbf, kf));
             A.new_hi[e] = T(hi);
             A.new_lo[e] = T(lo);
         }
@@ -555,8 +553,14 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         int lx0, lx1, ly0, ly1;
         region_of<OPX>(x0, x1, nx, lx0, lx1);
         region_of<OPY>(y0, y1, ny, ly0, ly1);
-        const T* q = A.u_in + B.q_off;
+        // Everything later phases need from the block and instance descriptors is read here,
+        // once: the global stores of phase 2 would otherwise force the compiler to reload it.
+        const int64_t qoff = B.q_off;
+        const T* q = A.u_in + qoff;
         const T* mt = A.met + B.m_off;
+        const InstanceDev& I = A.inst[B.instance];
+        const double cb = I.cb[A.stage];
+        const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
 
         // ---------------- phase 1: pointwise quantities ----------------
         // Stage this thread's phase-2 operands (detJ, RK state) into shared memory; the copies
@@ -576,7 +580,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                         for (int a = 0; a < nsrc; ++a)
 #pragma unroll
                             for (int cc = 0; cc < 4; ++cc)
-                                cp_async_elem(slot + (1 + 4 * a + cc) * TY * kTileX, src[a] + B.q_off + cc * np + pt);
+                                cp_async_elem(slot + (1 + 4 * a + cc) * TY * kTileX, src[a] + qoff + cc * np + pt);
                     }
             }
         }
@@ -616,7 +620,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         // full vector.
         const int r0 = y0 + warp * R;  // first global row of this thread
         const int nrows = min(R, y1 - r0);
-        const InstanceDev& I = A.inst[B.instance];
         if (lane < tw && nrows > 0) {
             const int col = x0 + lane;
             const T idxx = sizeof(T) == 8 ? T(B.idx_xi) : T(B.idx_xi_f);
@@ -625,6 +628,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
             const bool eta_interior = r0 >= OpShape<OPY>::M && r0 + R <= ny - OpShape<OPY>::M;
             const bool edge_col = col == 0 || col == nx - 1;
             const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
+            const float cbf = float(cb), caf = float(ca);
             T detj[R];
 #pragma unroll
             for (int u = 0; u < R; ++u) {
@@ -655,11 +659,12 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                         if (edge_col || row == 0 || row == ny - 1)
                             sK[cc * edge_slots(TY) + edge_slot(row, col, y0, x0, nx, ny, TY)] = kc;
                         else if constexpr (COMP)
-                            rk_update_staged<T>(A, I, B.q_off + row * nx + col + cc * np, q[cc * np + row * nx + col], kc,
-                                                [&](int a) { return sR[((1 + 4 * a + cc) * TY + row - y0) * kTileX + lane]; });
+                            rk_update_staged<T>(A, qoff + cc * np + row * nx + col, cbf, caf, kc, [&](int a) {
+                                return sR[((1 + 4 * a + cc) * TY + row - y0) * kTileX + lane];
+                            });
                         else
-                            rk_update<T, COMP>(A, I, B.q_off + row * nx + col, np, cc, q[cc * np + row * nx + col],
-                                               kc);
+                            rk_update<T, COMP>(A, qoff + cc * np + row * nx + col, q[cc * np + row * nx + col], kc,
+                                               cb, ca);
                     }
                 }
             }
@@ -693,7 +698,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                 }
                 sat_edge<T>(A, I, B, row, col, pt, yv, kv);
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, I, B.q_off + pt, np, cc, T(yv[cc]), T(kv[cc]));
+                for (int cc = 0; cc < 4; ++cc)
+                    rk_update<T, COMP>(A, qoff + cc * np + pt, T(yv[cc]), T(kv[cc]), cb, ca);
             }
         }
         // No barrier here: phase 3 reads only sK and global memory, and the next tile's phase 1
