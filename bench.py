@@ -336,7 +336,7 @@ def run_ours(args):
 
     peak, peak_kind = measured_hbm_peak()
     bpp = BYTES_PER_POINT_UPDATE["f32c"]
-    launches_stage = 4 * (s32.launches_per_step() - 1) // 4
+    launches_stage = (s32.launches_per_step() - 1) // 2  # a stage kernel and an edge kernel per group and stage
     bytes_per_launch = bpp * points / 4.0  # average over the 4 stage launches of a step
     achieved = bpp * points / (ms_step / 1e3) / 1e9
     traffic = recorded_traffic("f32c")

@@ -202,7 +202,8 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads);
 sbp_status sbp_system_set_stream(sbp_system* sys, void* stream);
 /* Device pointer to one block's current state plane set (f64 or f32 hi), for zero-copy use. */
 sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q);
-/* Kernel launches per RK4 step (the stage kernels plus the time update). */
+/* Kernel launches per RK4 step: per operator pair and stage a stage kernel and an edge (SAT)
+ * kernel, plus the time update. */
 int sbp_system_launches_per_step(const sbp_system* sys);
 
 #ifdef __cplusplus

@@ -26,10 +26,21 @@ struct BlockDev {
     int bc_kind[4];
     int bc_nb[4];
     int64_t q_off, m_off, x_off;
+    int64_t e_off;  // slot of this block's first edge point in the edge-k buffer (see edge_index)
     double idx_xi, idx_eta;  // 1/(1/(n-1)) per direction, f64
     float idx_xi_f, idx_eta_f;
     double hi_xi, hi_eta;  // SAT penalty (n-1)/H_0 (euler/src/lib.rs:1033-1037)
 };
+
+// Position of edge point (row, col) among a block's 2 nx + 2 ny - 4 edge points: the first row,
+// the last row, then the first and the last column without their corner points.
+__host__ __device__ __forceinline__ int edge_index(int row, int col, int nx, int ny) {
+    if (row == 0) return col;
+    if (row == ny - 1) return nx + col;
+    if (col == 0) return 2 * nx + row - 1;
+    return 2 * nx + ny - 2 + row - 1;  // col == nx - 1
+}
+__host__ __device__ constexpr int64_t edge_count(int64_t nx, int64_t ny) { return 2 * nx + 2 * ny - 4; }
 
 struct InstanceDev {
     double dt, time;

@@ -12,4 +12,7 @@ const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_u4(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_u9(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty);
+// Edge (SAT) kernel entries, one per precision.
+const void* sat_ptr_f64();
+const void* sat_ptr_f32();
 }  // namespace sbp

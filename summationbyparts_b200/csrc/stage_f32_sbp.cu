@@ -1,4 +1,4 @@
-// Instantiations of the fused stage kernel: SBP4/SBP8 operator pairs, compensated f32 state.
+// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs and of the edge (SAT) kernel, compensated f32 state.
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
 
@@ -15,5 +15,7 @@ const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty) {
     CASE(SBP8, SBP8, false, 32)
     return nullptr;
 }
+
+const void* sat_ptr_f32() { return reinterpret_cast<const void*>(&sat_kernel<float, true>); }
 
 }  // namespace sbp

@@ -1,4 +1,4 @@
-// Instantiations of the fused stage kernel: SBP4/SBP8 operator pairs, f64 state (reference arithmetic, built with -fmad=false).
+// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs and of the edge (SAT) kernel, f64 state (reference arithmetic, built with -fmad=false).
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
 
@@ -15,5 +15,7 @@ const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty) {
     CASE(SBP8, SBP8, false, 32)
     return nullptr;
 }
+
+const void* sat_ptr_f64() { return reinterpret_cast<const void*>(&sat_kernel<double, false>); }
 
 }  // namespace sbp

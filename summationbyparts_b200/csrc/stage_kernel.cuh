@@ -2,16 +2,21 @@
 //
 // One launch computes, for every point of every scheduled tile, the Euler right-hand side
 //   k = ((-dE/dxi - dF/deta) + diss_xi(alpha_u q) + diss_eta(alpha_v q)) / detJ
-// (RHS_upwind, euler/src/lib.rs:571-616; RHS_trad 483-515 without the dissipation terms),
-// adds the characteristic SATs on block edges in the order north, south, east, west
-// (SAT_characteristics, euler/src/lib.rs:1002-1013), and performs this stage's share of the
-// RK4 update (integrate::<Rk4>, utils/integrate/src/lib.rs:176-222):
+// (RHS_upwind, euler/src/lib.rs:571-616; RHS_trad 483-515 without the dissipation terms) and
+// performs this stage's share of the RK4 update (integrate::<Rk4>,
+// utils/integrate/src/lib.rs:176-222):
 //   stage 0: acc  = prev + (b0 dt) k ; next = prev + (a dt) k
 //   stage 1: acc += (b1 dt) k        ; next = prev + (a dt) k
 //   stage 2: acc += (b2 dt) k        ; next = prev + (a dt) k
 //   stage 3: new  = acc + (b3 dt) k
 // which is the reference's sequence fut = prev; fut += b_j dt k_j (j = 0..3) evaluated
-// incrementally, so the k_j never go to memory.
+// incrementally, so the k_j of interior points never go to memory.  Points on a block edge
+// store their k in the edge-k buffer instead; the edge kernel (sat_kernel, launched right after
+// on the same stream) adds the characteristic SATs in the order north, south, east, west
+// (SAT_characteristics, euler/src/lib.rs:1002-1013) and does their update.  The SAT of one
+// point is a long dependent f64 chain (vortex data, two hypot, a dozen divisions); evaluated by
+// a few threads of a tile it held the whole CTA at the next barrier, in a launch of its own it
+// runs one thread per edge point.
 //
 // Work decomposition.  A persistent grid of 256-thread CTAs walks a list of (block, y0, x0)
 // output tiles of TY rows x 32 columns.  Lane = column, warp w owns rows w*R .. w*R+R-1
@@ -55,6 +60,7 @@ struct StageArgs {
     T* u_out;                // next stage input (stages 0..2)
     T* new_hi;               // new state (stage 3)
     T* new_lo;
+    T* kedge;                // k of block-edge points, 4 per point (edge_index order per block)
     const T* met;            // metric planes in T
     const double* met64;     // metric planes in f64 (SAT terms)
     const double* xy;        // coordinates
@@ -79,16 +85,6 @@ constexpr int region_extent(int T, int H, int M, int N) {
     return a > N ? a : N;
 }
 
-// Block-edge points of one tile get a slot each for their parked k: the first and last block
-// row (32 slots each, by column) and the first and last block column (TY slots each, by row).
-__host__ __device__ constexpr int edge_slots(int TY) { return 2 * kTileX + 2 * TY; }
-__device__ __forceinline__ int edge_slot(int row, int col, int y0, int x0, int nx, int ny, int TY) {
-    if (row == 0) return col - x0;
-    if (row == ny - 1) return kTileX + (col - x0);
-    if (col == 0) return 2 * kTileX + (row - y0);
-    return 2 * kTileX + TY + (row - y0);  // col == nx - 1
-}
-
 // Shared-memory geometry of one tile: xi arrays are TY rows x XP columns, eta arrays HYP rows
 // x 32 columns.
 template <int OPX, int OPY, int TY>
@@ -107,7 +103,7 @@ __host__ __device__ constexpr int staged_elems(bool comp, int TY) { return comp 
 template <int OPX, int OPY, int TY, class T>
 constexpr size_t stage_smem(bool upw, bool comp) {
     using G = StageGeom<OPX, OPY, TY>;
-    return sizeof(T) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * edge_slots(TY) + staged_elems(comp, TY));
+    return sizeof(T) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + staged_elems(comp, TY));
 }
 
 // Characteristic SAT of one edge point (euler/src/lib.rs:1150-1252), f64, written row by row
@@ -536,8 +532,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sE = reinterpret_cast<T*>(smem_raw);       // [UPW ? 8 : 4][TY][XP]: Ehat (0..3), alpha_u q (4..7)
     T* sF = sE + (UPW ? 8 : 4) * XA;              // [UPW ? 8 : 4][HYP][32]: Fhat (0..3), alpha_v q (4..7)
-    T* sK = sF + (UPW ? 8 : 4) * YA;              // [4][64 + 2 TY]: k of block-edge points awaiting the SAT
-    T* sR = sK + 4 * edge_slots(TY);              // [13][TY][32]: staged phase-2 operands (COMP)
+    T* sR = sF + (UPW ? 8 : 4) * YA;              // [13][TY][32]: staged phase-2 operands (COMP)
     const T gamma = T(A.gamma);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned bad = 0;
@@ -555,7 +550,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         region_of<OPY>(y0, y1, ny, ly0, ly1);
         // Everything later phases need from the block and instance descriptors is read here,
         // once: the global stores of phase 2 would otherwise force the compiler to reload it.
-        const int64_t qoff = B.q_off;
+        const int64_t qoff = B.q_off, eoff = B.e_off;
         const T* q = A.u_in + qoff;
         const T* mt = A.met + B.m_off;
         const InstanceDev& I = A.inst[B.instance];
@@ -616,8 +611,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
 
         // ---------------- phase 2: stencils and stage update ----------------
         // Interior points finish component by component (k_c, then the RK update of c); points
-        // on a block edge park their k in shared memory for phase 3, where the SAT sees the
-        // full vector.
+        // on a block edge store k_c for the edge kernel.
         const int r0 = y0 + warp * R;  // first global row of this thread
         const int nrows = min(R, y1 - r0);
         if (lane < tw && nrows > 0) {
@@ -657,7 +651,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                         if constexpr (UPW) kc = (-ex[cc][u] - dF[u] + dx[cc][u] + ay[u]) / detj[u];
                         else kc = (-ex[cc][u] - dF[u]) / detj[u];
                         if (edge_col || row == 0 || row == ny - 1)
-                            sK[cc * edge_slots(TY) + edge_slot(row, col, y0, x0, nx, ny, TY)] = kc;
+                            A.kedge[4 * (eoff + edge_index(row, col, nx, ny)) + cc] = kc;
                         else if constexpr (COMP)
                             rk_update_staged<T>(A, qoff + cc * np + row * nx + col, cbf, caf, kc, [&](int a) {
                                 return sR[((1 + 4 * a + cc) * TY + row - y0) * kTileX + lane];
@@ -669,45 +663,40 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                 }
             }
         }
+        // Every thread is done with this tile's shared arrays before the next tile's phase 1.
         __syncthreads();
-
-        // ---------------- phase 3: SATs of the tile's block-edge points ----------------
-        // One thread per edge slot: first/last block row (by column), first/last block column
-        // (by row, rows 0 and ny-1 excluded: they already own a row slot).
-        {
-            const int s_ = threadIdx.x;
-            int row = -1, col = 0;
-            if (s_ < kTileX) {
-                if (y0 == 0 && s_ < tw) row = 0, col = x0 + s_;
-            } else if (s_ < 2 * kTileX) {
-                if (y1 == ny && s_ - kTileX < tw) row = ny - 1, col = x0 + s_ - kTileX;
-            } else if (s_ < 2 * kTileX + TY) {
-                const int r = y0 + s_ - 2 * kTileX;
-                if (x0 == 0 && r < y1 && r != 0 && r != ny - 1) row = r, col = 0;
-            } else if (s_ < edge_slots(TY)) {
-                const int r = y0 + s_ - 2 * kTileX - TY;
-                if (x1 == nx && r < y1 && r != 0 && r != ny - 1) row = r, col = nx - 1;
-            }
-            if (row >= 0) {
-                const int pt = row * nx + col;
-                double yv[4], kv[4];
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    yv[cc] = double(q[cc * np + pt]);
-                    kv[cc] = double(sK[cc * edge_slots(TY) + s_]);
-                }
-                sat_edge<T>(A, I, B, row, col, pt, yv, kv);
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc)
-                    rk_update<T, COMP>(A, qoff + cc * np + pt, T(yv[cc]), T(kv[cc]), cb, ca);
-            }
-        }
-        // No barrier here: phase 3 reads only sK and global memory, and the next tile's phase 1
-        // writes only the xi/eta arrays (whose readers all passed the barrier after phase 2);
-        // sK is rewritten only in the next tile's phase 2, behind the next barrier.  The edge
-        // threads' SAT work overlaps the other threads' next phase 1.
     }
     if (bad) atomicOr(A.status, bad);
+}
+
+// Edge kernel: one thread per block-edge point of a stage launch's blocks (edges[i] = block,
+// row, col).  Adds the SATs to the k the stage kernel stored and does the point's RK update.
+constexpr int kSatThreads = 128;
+template <class T, bool COMP>
+__global__ void __launch_bounds__(kSatThreads) sat_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
+                                                          int nedges) {
+    const int i = blockIdx.x * kSatThreads + threadIdx.x;
+    if (i >= nedges) return;
+    const int4 ed = edges[i];
+    const BlockDev& B = A.blocks[ed.x];
+    const InstanceDev& I = A.inst[B.instance];
+    const int row = ed.y, col = ed.z;
+    const int nx = B.nx, ny = B.ny;
+    const int64_t np = B.npad, qoff = B.q_off;
+    const int64_t slot = 4 * (B.e_off + edge_index(row, col, nx, ny));
+    const double cb = I.cb[A.stage];
+    const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
+    const int pt = row * nx + col;
+    const T* q = A.u_in + qoff;
+    double yv[4], kv[4];
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) {
+        yv[cc] = double(q[cc * np + pt]);
+        kv[cc] = double(A.kedge[slot + cc]);
+    }
+    sat_edge<T>(A, I, B, row, col, pt, yv, kv);
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, qoff + cc * np + pt, T(yv[cc]), T(kv[cc]), cb, ca);
 }
 
 }  // namespace sbp

@@ -60,7 +60,7 @@ size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
     const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
     const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
     const size_t elems =
-        (size_t)(4 * ty * xp + 4 * hyp * kTileX) * (upw ? 2 : 1) + 4 * edge_slots(ty) + staged_elems(prec == 1, ty);
+        (size_t)(4 * ty * xp + 4 * hyp * kTileX) * (upw ? 2 : 1) + staged_elems(prec == 1, ty);
     return elems * (prec == 0 ? sizeof(double) : sizeof(float));
 }
 
@@ -70,6 +70,8 @@ struct Group {
     const void* fn;
     int4* d_tiles = nullptr;
     int ntiles = 0;
+    int4* d_edges = nullptr;  // (block, row, col) of every edge point of the group's blocks
+    int nedges = 0;
     int WX = 0, HY = 0;
     size_t smem = 0;
     int grid = 0;
@@ -112,6 +114,8 @@ struct sbp_system {
     double* d_sums = nullptr;
     unsigned long long* d_speeds = nullptr;
     void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
+    void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
+    int64_t nedge = 0;
     // schedule
     int TY = 16, TX = kTileX, threads = kStageThreads;
     std::vector<int> active;
@@ -133,7 +137,10 @@ struct sbp_system {
 namespace {
 
 void free_groups(sbp_system* s) {
-    for (auto& g : s->groups) cudaFree(g.d_tiles);
+    for (auto& g : s->groups) {
+        cudaFree(g.d_tiles);
+        cudaFree(g.d_edges);
+    }
     s->groups.clear();
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
@@ -149,7 +156,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef};
+                    s->d_coef,   s->kedge};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -213,6 +220,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.met64 = s->met64;
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
+    a.kedge = static_cast<T*>(s->kedge);
     a.gamma = s->gamma;
     a.status = s->status;
     return a;
@@ -221,14 +229,22 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
 sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st) {
     if (g.ntiles == 0) return SBP_OK;
     cudaError_t e;
+    const void* sat = s->prec == 0 ? sat_ptr_f64() : sat_ptr_f32();
+    const dim3 sat_grid((g.nedges + kSatThreads - 1) / kSatThreads);
+    int4* edges = g.d_edges;
+    int nedges = g.nedges;
     if (s->prec == 0) {
         StageArgs<double> a = stage_args<double>(s, stage, g);
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     } else {
         StageArgs<float> a = stage_args<float>(s, stage, g);
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     }
     return cuda_status(e, "stage kernel launch");
 }
@@ -261,7 +277,7 @@ sbp_status build_schedule(sbp_system* s) {
             gp = &s->groups.back();
         }
     }
-    std::vector<std::vector<int4>> tiles(s->groups.size());
+    std::vector<std::vector<int4>> tiles(s->groups.size()), edges(s->groups.size());
     for (int b = 0; b < s->nblocks; ++b) {
         const BlockDev& B = s->hb[b];
         if (!s->active[B.instance]) continue;
@@ -282,6 +298,11 @@ sbp_status build_schedule(sbp_system* s) {
                 g.HY = std::max(g.HY, hi - lo);
                 tiles[gi].push_back(make_int4(b, y0, x0, 0));
             }
+        // edge points in edge_index order: first row, last row, first column, last column
+        for (int c = 0; c < B.nx; ++c) edges[gi].push_back(make_int4(b, 0, c, 0));
+        for (int c = 0; c < B.nx; ++c) edges[gi].push_back(make_int4(b, B.ny - 1, c, 0));
+        for (int r = 1; r < B.ny - 1; ++r) edges[gi].push_back(make_int4(b, r, 0, 0));
+        for (int r = 1; r < B.ny - 1; ++r) edges[gi].push_back(make_int4(b, r, B.nx - 1, 0));
     }
     for (size_t gi = 0; gi < s->groups.size(); ++gi) {
         Group& g = s->groups[gi];
@@ -314,6 +335,10 @@ sbp_status build_schedule(sbp_system* s) {
         if (g.ntiles) {
             SBP_TRY_CUDA(cudaMalloc(&g.d_tiles, g.ntiles * sizeof(int4)));
             SBP_TRY_CUDA(cudaMemcpyAsync(g.d_tiles, tiles[gi].data(), g.ntiles * sizeof(int4),
+                                         cudaMemcpyHostToDevice, s->stream));
+            g.nedges = (int)edges[gi].size();
+            SBP_TRY_CUDA(cudaMalloc(&g.d_edges, g.nedges * sizeof(int4)));
+            SBP_TRY_CUDA(cudaMemcpyAsync(g.d_edges, edges[gi].data(), g.nedges * sizeof(int4),
                                          cudaMemcpyHostToDevice, s->stream));
         }
     }
@@ -500,6 +525,8 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         B.q_off = s->nq;
         B.m_off = s->nm;
         B.x_off = s->nx2;
+        B.e_off = s->nedge;
+        s->nedge += edge_count(D.nx, D.ny);
         s->nq += 4 * (int64_t)B.npad;
         s->nm += 5 * (int64_t)B.npad;
         s->nx2 += 2 * (int64_t)B.npad;
@@ -553,6 +580,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_sums, nblocks * sizeof(double));
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
+    e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
     cudaStream_t st = s->stream;
     e = e ?: cudaMemsetAsync(s->prev_hi, 0, s->nq * ts, st);
@@ -1034,9 +1062,9 @@ int sbp_system_launches_per_step(const sbp_system* sys) {
             auto p = std::make_pair(B.op_xi, B.op_eta);
             if (std::find(pairs.begin(), pairs.end(), p) == pairs.end()) pairs.push_back(p);
         }
-        return 4 * (int)pairs.size() + 1;
+        return 8 * (int)pairs.size() + 1;
     }
-    return 4 * (int)sys->groups.size() + 1;
+    return 8 * (int)sys->groups.size() + 1;
 }
 
 }  // extern "C"
