@@ -175,13 +175,13 @@ __device__ __forceinline__ void sat_point_rows(double gamma, const double y[4], 
 }
 
 // Pointwise quantities of one point (fluxes, euler/src/lib.rs:680-735; upwind_dissipation
-// 619-674).  Writes the xi-direction values (Ehat, alpha_u q) and/or eta-direction values
-// (Fhat, alpha_v q) into shared memory at the given slots.
+// 619-674) from its state qv and metrics m = (dxi/dx, dxi/dy, deta/dx, deta/dy), each times
+// detJ.  Writes the xi-direction values (Ehat, alpha_u q) and/or eta-direction values (Fhat,
+// alpha_v q) into shared memory at the given slots.
 template <class T, bool UPW, bool EXACT>
-__device__ __forceinline__ void pointwise(const T* __restrict__ q, const T* __restrict__ mt, int64_t np, int pt,
-                                          T gamma, T* sxi, int xa, T* seta, int ya, bool want_xi, bool want_eta,
-                                          unsigned& bad) {
-    const T rho = __ldg(q + pt), rhou = __ldg(q + np + pt), rhov = __ldg(q + 2 * np + pt), e = __ldg(q + 3 * np + pt);
+__device__ __forceinline__ void pointwise(const T qv[4], const T m[4], T gamma, T* sxi, int xa, T* seta, int ya,
+                                          bool want_xi, bool want_eta, unsigned& bad) {
+    const T rho = qv[0], rhou = qv[1], rhov = qv[2], e = qv[3];
     T E[4], F[4];
     T p_, u = T(0), v = T(0), c = T(0);
     if constexpr (EXACT) {
@@ -218,7 +218,7 @@ __device__ __forceinline__ void pointwise(const T* __restrict__ q, const T* __re
         if (!(p_ > T(0))) bad |= STATUS_P;
     }
     if (want_xi) {
-        const T jxx = __ldg(mt + np + pt), jxy = __ldg(mt + 2 * np + pt);
+        const T jxx = m[0], jxy = m[1];
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) sxi[cc * xa] = jxx * E[cc] + jxy * F[cc];
         if constexpr (UPW) {
@@ -232,7 +232,7 @@ __device__ __forceinline__ void pointwise(const T* __restrict__ q, const T* __re
         }
     }
     if (want_eta) {
-        const T jyx = __ldg(mt + 3 * np + pt), jyy = __ldg(mt + 4 * np + pt);
+        const T jyx = m[2], jyy = m[3];
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) seta[cc * ya] = jyx * E[cc] + jyy * F[cc];
         if constexpr (UPW) {
@@ -529,6 +529,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
     using G = StageGeom<OPX, OPY, TY>;
     constexpr int R = TY / kStageWarps;
     constexpr int XA = G::XA, YA = G::YA, XP = G::XP;
+    constexpr int P1B = sizeof(T) == 4 ? 4 : 2;  // phase-1 points per thread and batch
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sE = reinterpret_cast<T*>(smem_raw);       // [UPW ? 8 : 4][TY][XP]: Ehat (0..3), alpha_u q (4..7)
     T* sF = sE + (UPW ? 8 : 4) * XA;              // [UPW ? 8 : 4][HYP][32]: Fhat (0..3), alpha_v q (4..7)
@@ -582,29 +583,61 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
 
         // One index space over all threads: eta-region points (rows ly0..ly1, 32 slots per row,
         // slots >= tw idle) followed by the xi-halo points (tile rows x hw columns, packed).
+        // A thread takes points p = tid, tid + 256, ... in batches of P1B: all loads of a batch
+        // are issued before any of its points is evaluated, so a thread waits for memory once
+        // per batch rather than once per point.
         const int eh = ly1 - ly0;
         const int hl = x0 - lx0, hw = hl + (lx1 - x1);
         const int n_eta = eh * kTileX, n_all = n_eta + th * hw;
         const unsigned hw_inv = hw ? (65536u + hw - 1) / hw : 0u;  // exact floor(h / hw) for h < 1024
-        for (int p = threadIdx.x; p < n_all; p += kStageThreads) {
-            if (p < n_eta) {
-                const int row = ly0 + (p >> 5), tx = p & 31;
-                if (tx < tw) {
-                    const int col = x0 + tx;
-                    const bool in_tile = row >= y0 && row < y1;
-                    pointwise<T, UPW, !COMP>(q, mt, np, row * nx + col, gamma,
-                                      in_tile ? sE + (row - y0) * XP + (col - lx0) : nullptr, XA,
-                                      sF + (row - ly0) * kTileX + tx, YA, in_tile, true, bad);
+        for (int pb = threadIdx.x; pb < n_all; pb += P1B * kStageThreads) {
+            int pt[P1B], oxi[P1B], oeta[P1B];  // point, xi slot (-1: none), eta slot (-1: none)
+            T qv[P1B][4], m[P1B][4];
+#pragma unroll
+            for (int b = 0; b < P1B; ++b) {
+                const int p = pb + b * kStageThreads;
+                pt[b] = -1;
+                oxi[b] = -1;
+                oeta[b] = -1;
+                if (p < n_eta) {
+                    const int row = ly0 + (p >> 5), tx = p & 31;
+                    if (tx < tw) {
+                        const int col = x0 + tx;
+                        pt[b] = row * nx + col;
+                        oeta[b] = (row - ly0) * kTileX + tx;
+                        if (row >= y0 && row < y1) oxi[b] = (row - y0) * XP + (col - lx0);
+                    }
+                } else if (p < n_all) {
+                    const int h = p - n_eta;
+                    const int ty = (int)(((unsigned)h * hw_inv) >> 16);
+                    const int hc = h - ty * hw;
+                    const int col = hc < hl ? lx0 + hc : x1 + (hc - hl);
+                    pt[b] = (y0 + ty) * nx + col;
+                    oxi[b] = ty * XP + (col - lx0);
                 }
-            } else {
-                const int h = p - n_eta;
-                const int ty = (int)(((unsigned)h * hw_inv) >> 16);
-                const int hc = h - ty * hw;
-                const int row = y0 + ty;
-                const int col = hc < hl ? lx0 + hc : x1 + (hc - hl);
-                pointwise<T, UPW, !COMP>(q, mt, np, row * nx + col, gamma, sE + ty * XP + (col - lx0), XA, nullptr, YA,
-                                  true, false, bad);
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    qv[b][cc] = T(1);
+                    m[b][cc] = T(0);
+                }
+                if (pt[b] >= 0) {
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) qv[b][cc] = __ldg(q + cc * np + pt[b]);
+                    if (oxi[b] >= 0) {
+                        m[b][0] = __ldg(mt + np + pt[b]);
+                        m[b][1] = __ldg(mt + 2 * np + pt[b]);
+                    }
+                    if (oeta[b] >= 0) {
+                        m[b][2] = __ldg(mt + 3 * np + pt[b]);
+                        m[b][3] = __ldg(mt + 4 * np + pt[b]);
+                    }
+                }
             }
+#pragma unroll
+            for (int b = 0; b < P1B; ++b)
+                if (pt[b] >= 0)
+                    pointwise<T, UPW, !COMP>(qv[b], m[b], gamma, sE + (oxi[b] >= 0 ? oxi[b] : 0), XA,
+                                             sF + (oeta[b] >= 0 ? oeta[b] : 0), YA, oxi[b] >= 0, oeta[b] >= 0, bad);
         }
         if constexpr (COMP) cp_async_wait_all();
         __syncthreads();
