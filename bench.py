@@ -29,12 +29,16 @@ UNIT = "point-updates/s"
 # Algorithmic HBM bytes per point-update of the fused stage design (sum over the 4 stage
 # launches of the state, accumulator and metric planes each launch must read and write once).
 BYTES_PER_POINT_UPDATE = {"f32c": 464, "f64": 672}
+# The same per stage launch (stage 0..3): stage 0 reads the step-start state (and its low part)
+# and the metrics and writes the accumulator and the next stage input; stages 1 and 2 also read
+# the accumulator and the step-start state; stage 3 reads the accumulator and writes the new state.
+BYTES_PER_POINT_STAGE = {"f32c": (100, 132, 132, 100), "f64": (136, 200, 200, 136)}
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=300)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--ninst", type=int, default=512)
@@ -44,6 +48,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--tiles", default="", help="TY,TX,THREADS: fixed tile schedule instead of the autotuner")
+    p.add_argument("--kernel-reps", type=int, default=5, help="repetitions of the per-kernel timing")
+    p.add_argument("--kernel-only", action="store_true",
+                   help="only the per-kernel timing of the stage kernels (for profiling runs)")
     return p.parse_args()
 
 
@@ -147,6 +154,43 @@ def timed_advance(torch, s, stream, steps, barrier):
     return e0.elapsed_time(e1)
 
 
+def kernel_timing(torch, s, stream, precision, reps):
+    """Stage-kernel roofline: every group's stage kernel for each RK4 stage, launched one at a
+    time and timed with CUDA events on the system's stream.  Returns algorithmic bytes / kernel
+    time over all those launches and the per-launch detail.  Leaves the stage buffers as the
+    launches leave them (the system must be re-initialised before its results mean anything)."""
+    groups = s.groups()
+    per_stage = BYTES_PER_POINT_STAGE[precision]
+    for g in range(len(groups)):  # warm-up
+        for st in range(4):
+            s.launch_stage(g, st)
+    torch.cuda.synchronize()
+    ev = []
+    for _ in range(reps):
+        for g, (_, _, pts) in enumerate(groups):
+            for st in range(4):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                s.launch_stage(g, st)
+                b.record(stream)
+                ev.append((g, st, pts, a, b))
+    torch.cuda.synchronize()
+    total_bytes = total_ms = 0.0
+    detail = {}
+    for g, st, pts, a, b in ev:
+        ms = a.elapsed_time(b)
+        total_bytes += per_stage[st] * pts
+        total_ms += ms
+        key = f"group{g}_stage{st}"
+        detail.setdefault(key, []).append(ms)
+    launches = [{"group": g, "op_xi": groups[g][0], "op_eta": groups[g][1], "points": groups[g][2], "stage": st,
+                 "algorithmic_bytes": per_stage[st] * groups[g][2],
+                 "ms_median": statistics.median(detail[f"group{g}_stage{st}"])}
+                for g in range(len(groups)) for st in range(4)]
+    return total_bytes / (total_ms / 1e3) / 1e9, total_ms / len(ev), launches
+
+
 def cpu_baseline(insts, seconds, nthreads, steps_per_sample=1):
     """The oracle (C++ port of the reference arithmetic) on the host cores: time one step of a
     bounded sample of instances, all threads.  Returns (point-updates/s, description)."""
@@ -245,6 +289,16 @@ def run_ours(args):
         tiles = fixed
     else:
         tiles = s32.autotune()
+    if args.kernel_only:
+        s32.advance(1)
+        gbs, ms_launch, launches = kernel_timing(torch, s32, stream, "f32c", args.kernel_reps)
+        if rank == 0:
+            print(json.dumps({"kernel": "stage_kernel", "achieved_gbs": gbs, "ms_per_launch": ms_launch,
+                              "launches": launches, "tiles": list(tiles), "points": points}), flush=True)
+        s32.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     for _ in range(args.warmup):
         s32.advance(1)
     clocks = Clocks(local)
@@ -307,6 +361,15 @@ def run_ours(args):
                "d2h_bytes_per_step": n * 8, "steps": ke,
                "path": "sbp_system_set_state_all + sbp_system_advance(1) + sbp_system_get_state_all, f64 host state"}
 
+    # per-kernel roofline of the stage kernels, with every instance active (the accuracy run
+    # below re-initialises both systems)
+    k64 = None
+    if s64 is not None:
+        k64, _, _ = kernel_timing(torch, s64, stream, "f64", args.kernel_reps)
+        if fp64 is not None:
+            fp64["stage_kernel_achieved_gbs"] = k64
+    achieved, ms_launch, klaunch = kernel_timing(torch, s32, stream, "f32c", args.kernel_reps)
+
     # same-error check: every instance of both forms to t = 2 (ragged step counts)
     if s64 is not None and not args.no_accuracy:
         import numpy as np
@@ -331,6 +394,14 @@ def run_ours(args):
                "l2_err_vs_exact_f32c_median": float(np.median(e32)), "l2_err_vs_exact_f32c_max": float(e32.max()),
                "err_rel_diff_f32c_vs_f64_max": float(rel.max()),
                "state_rel_l2_f32c_vs_f64": (a - b).norm().item() / b.norm().item()}
+        # per instance (one block each, packed (4, side, side) in instance order)
+        per, off = [], 0
+        for inst in insts:
+            m = 4 * inst.side * inst.side
+            per.append((a[off:off + m] - b[off:off + m]).norm().item() / b[off:off + m].norm().item())
+            off += m
+        acc["state_rel_l2_f32c_vs_f64_per_instance_median"] = float(np.median(per))
+        acc["state_rel_l2_f32c_vs_f64_per_instance_max"] = float(np.max(per))
     if s64 is not None:
         s64.close()
 
@@ -338,13 +409,18 @@ def run_ours(args):
     bpp = BYTES_PER_POINT_UPDATE["f32c"]
     launches_stage = (s32.launches_per_step() - 1) // 2  # a stage kernel and an edge kernel per group and stage
     bytes_per_launch = bpp * points / 4.0  # average over the 4 stage launches of a step
-    achieved = bpp * points / (ms_step / 1e3) / 1e9
     traffic = recorded_traffic("f32c")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (traffic * points / 4.0) if traffic else None,
-            "kernel": "stage_kernel (fused RK4 stage)", "algorithmic_bytes_per_point_update": bpp,
-            "bytes_per_launch": bytes_per_launch, "stage_launches_per_step": launches_stage,
-            "peak_source": f"{peak_kind} hbm_gbs"}
+            "kernel": "stage_kernel (fused RK4 stage, compensated f32)",
+            "achieved_from": "algorithmic bytes of every group's stage-kernel launch for stages 0-3, "
+                             "divided by their CUDA-event durations on the launching stream, "
+                             f"{args.kernel_reps} repetitions",
+            "ms_per_launch": ms_launch, "launches": klaunch,
+            "algorithmic_bytes_per_point_update": bpp, "bytes_per_launch": bytes_per_launch,
+            "stage_launches_per_step": launches_stage,
+            "whole_step_gbs": bpp * points / (ms_step / 1e3) / 1e9,
+            "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth, burst)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -206,6 +206,20 @@ sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q);
  * kernel, plus the time update. */
 int sbp_system_launches_per_step(const sbp_system* sys);
 
+/* Per-kernel measurement.  A system's blocks are scheduled in groups, one per operator pair
+ * (xi, eta); each group has one stage-kernel launch per RK4 stage.  No counterpart in the
+ * reference (its RHS is a sequence of CPU sweeps); these exist so a caller can time one kernel
+ * with events on the system's stream. */
+/* Number of groups (builds the schedule if needed); -1 on error. */
+int sbp_system_group_count(sbp_system* sys);
+/* Operator pair and grid points of one group. */
+sbp_status sbp_system_group_info(sbp_system* sys, int group, int* op_xi, int* op_eta, int64_t* points);
+/* Enqueue one group's stage kernel for RK4 stage 0..3 on the system's stream, followed by its
+ * edge (SAT) kernel when with_edges != 0.  This advances no time and checks no status: it runs
+ * the stage on whatever the stage buffers hold, so a system used for it must be re-initialised
+ * before its results mean anything. */
+sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int with_edges);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,9 @@ SIGNATURES = {
     "sbp_system_set_stream": (_i, [_vp, _vp]),
     "sbp_system_device_state": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
     "sbp_system_launches_per_step": (_i, [_vp]),
+    "sbp_system_group_count": (_i, [_vp]),
+    "sbp_system_group_info": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i64)]),
+    "sbp_system_launch_stage": (_i, [_vp, _i, _i, _i]),
 }
 
 

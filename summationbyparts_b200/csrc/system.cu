@@ -72,6 +72,7 @@ struct Group {
     int ntiles = 0;
     int4* d_edges = nullptr;  // (block, row, col) of every edge point of the group's blocks
     int nedges = 0;
+    int64_t points = 0;       // grid points of the group's blocks
     int WX = 0, HY = 0;
     size_t smem = 0;
     int grid = 0;
@@ -226,7 +227,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     return a;
 }
 
-sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st) {
+sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st, bool edges_too = true) {
     if (g.ntiles == 0) return SBP_OK;
     cudaError_t e;
     const void* sat = s->prec == 0 ? sat_ptr_f64() : sat_ptr_f32();
@@ -238,13 +239,13 @@ sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t s
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
-        if (e == cudaSuccess) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
+        if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     } else {
         StageArgs<float> a = stage_args<float>(s, stage, g);
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
-        if (e == cudaSuccess) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
+        if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     }
     return cuda_status(e, "stage kernel launch");
 }
@@ -298,6 +299,7 @@ sbp_status build_schedule(sbp_system* s) {
                 g.HY = std::max(g.HY, hi - lo);
                 tiles[gi].push_back(make_int4(b, y0, x0, 0));
             }
+        g.points += (int64_t)B.nx * B.ny;
         // edge points in edge_index order: first row, last row, first column, last column
         for (int c = 0; c < B.nx; ++c) edges[gi].push_back(make_int4(b, 0, c, 0));
         for (int c = 0; c < B.nx; ++c) edges[gi].push_back(make_int4(b, B.ny - 1, c, 0));
@@ -1050,6 +1052,45 @@ sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q) {
     if (!sys || !d_q || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
     *d_q = static_cast<char*>(sys->prev_hi) + sys->hb[block].q_off * sys->tsize();
     return SBP_OK;
+}
+
+int sbp_system_group_count(sbp_system* sys) {
+    clear_error();
+    if (!sys) return -1;
+    cudaSetDevice(sys->device);
+    if (sys->sched_dirty && build_schedule(sys) != SBP_OK) return -1;
+    return (int)sys->groups.size();
+}
+
+sbp_status sbp_system_group_info(sbp_system* sys, int group, int* op_xi, int* op_eta, int64_t* points) {
+    clear_error();
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
+    if (group < 0 || group >= (int)sys->groups.size()) {
+        set_error("group %d out of range (%d groups)", group, (int)sys->groups.size());
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    const Group& g = sys->groups[group];
+    if (op_xi) *op_xi = g.opx;
+    if (op_eta) *op_eta = g.opy;
+    if (points) *points = g.points;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int with_edges) {
+    clear_error();
+    if (!sys || stage < 0 || stage > 3) {
+        set_error("bad system or stage %d", stage);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(sys->device);
+    if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
+    if (group < 0 || group >= (int)sys->groups.size()) {
+        set_error("group %d out of range (%d groups)", group, (int)sys->groups.size());
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    return launch_group(sys, stage, sys->groups[group], sys->st(), with_edges != 0);
 }
 
 int sbp_system_launches_per_step(const sbp_system* sys) {

@@ -135,6 +135,24 @@ class BlockSystem:
     def launches_per_step(self) -> int:
         return _capi.lib.sbp_system_launches_per_step(self.h)
 
+    # -- per-kernel measurement (sbp_system_group_* / sbp_system_launch_stage)
+    def groups(self) -> list[tuple[int, int, int]]:
+        """(op_xi, op_eta, points) of each stage-kernel group."""
+        n = _capi.lib.sbp_system_group_count(self.h)
+        if n < 0:
+            raise _capi.SbpError(1, _capi.lib.sbp_last_error().decode(errors='replace'))
+        out = []
+        for g in range(n):
+            ox, oy, pts = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+            check(_capi.lib.sbp_system_group_info(self.h, g, ctypes.byref(ox), ctypes.byref(oy), ctypes.byref(pts)))
+            out.append((ox.value, oy.value, pts.value))
+        return out
+
+    def launch_stage(self, group: int, stage: int, with_edges: bool = False) -> None:
+        """Enqueue one group's stage kernel (and optionally its edge kernel) on the system's
+        stream.  Advances no time; the stage buffers are left as the launch leaves them."""
+        check(_capi.lib.sbp_system_launch_stage(self.h, group, stage, int(with_edges)))
+
     # -- state
     def set_state(self, block: int, q: np.ndarray) -> None:
         q = np.ascontiguousarray(q, dtype=np.float64)

@@ -237,3 +237,34 @@ def test_interface_length_mismatch_rejected():
     with pytest.raises(SbpError) as e:
         BlockSystem(b, 1)
     assert e.value.status == 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32c"])
+def test_stage_launches_match_advance(precision):
+    """Launching every group's stage and edge kernels stage by stage (sbp_system_launch_stage)
+    gives the same state, bit for bit, as one graph-captured sbp_system_advance step; the groups
+    partition the blocks by operator pair."""
+    from summationbyparts_b200 import workloads
+    from summationbyparts_b200.system import BlockSystem
+    insts = [i for i in workloads.ensemble_instances(40, seed=1) if i.side <= 120][:4]
+    assert {i.op_id for i in insts} == {workloads.UPWIND4, workloads.UPWIND9}
+    out = []
+    for mode in ("advance", "launch"):
+        g = BlockSystem(workloads.ensemble_blocks(insts), len(insts), precision, 1.4)
+        for k, inst in enumerate(insts):
+            g.set_vortex(inst.vortex, k)
+            g.set_dt(inst.dt, k)
+        g.init_vortex(0.0)
+        groups = g.groups()
+        assert sorted((ox, oy) for ox, oy, _ in groups) == [(workloads.UPWIND4,) * 2, (workloads.UPWIND9,) * 2]
+        assert sum(p for _, _, p in groups) == sum(i.side ** 2 for i in insts)
+        if mode == "advance":
+            g.advance(1)
+        else:
+            for st in range(4):
+                for gi in range(len(groups)):
+                    g.launch_stage(gi, st, with_edges=True)
+        out.append(np.concatenate([g.state(b).ravel() for b in range(len(insts))]))
+        g.close()
+    assert out[0].tobytes() == out[1].tobytes()
