@@ -168,6 +168,9 @@ sbp_status sbp_system_get_state(sbp_system* sys, int block, double* q);
  * 2 x (4, ny, nx) f32 per block (hi then lo) when dtype = SBP_F32, else widened f64. */
 sbp_status sbp_system_set_state_all(sbp_system* sys, int dtype, const void* q);
 sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q);
+/* The same packing into device memory (sbp_system_state_count(dtype) elements of 8 bytes for
+ * SBP_F64, 4 for SBP_F32), for callers that keep the result on the GPU. */
+sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q);
 /* Number of state elements of sbp_system_{set,get}_state_all for dtype. */
 int64_t sbp_system_state_count(const sbp_system* sys, int dtype);
 
@@ -219,6 +222,53 @@ sbp_status sbp_system_group_info(sbp_system* sys, int group, int* op_xi, int* op
  * the stage on whatever the stage buffers hold, so a system used for it must be re-initialised
  * before its results mean anything. */
 sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int with_edges);
+
+/* ---------------------------------------------------------------------------------------
+ * Learned correction of a coarse solve (configuration 4).  No counterpart in the reference.
+ * A 5-layer 3x3 convolutional network (4 -> 32 -> 32 -> 32 -> 32 -> 4 channels, GELU between
+ * layers, zero padding) on the 64 x 64 coarse grid maps the coarse state at the end time to a
+ * correction toward the restriction of a fine-grid solve.  Activations BF16, accumulation FP32
+ * on the tensor cores, parameters and gradients FP32, Adam.  States are device arrays of
+ * images [n][4][64][64] (component planes), consecutive images img_stride elements apart.
+ * The network input is (state - in_mean) / in_scale per component, its output y the
+ * correction divided by out_scale; the loss is the mean squared error of y against
+ * (fine_restricted - coarse) / out_scale.
+ * ------------------------------------------------------------------------------------- */
+typedef struct sbp_cnn sbp_cnn;
+/* Network with activation buffers for up to max_batch images; parameters from seed. */
+sbp_status sbp_cnn_create(int device, int max_batch, unsigned long long seed, sbp_cnn** out);
+sbp_status sbp_cnn_destroy(sbp_cnn* net);
+/* Stream for all later work of the network (cudaStream_t; NULL = the legacy default stream).
+ * Until it is called the network uses a stream of its own. */
+sbp_status sbp_cnn_set_stream(sbp_cnn* net, void* stream);
+sbp_status sbp_cnn_synchronize(sbp_cnn* net);
+/* Number of FP32 parameters (padded layout: per layer weights [cout][9][cin], then biases). */
+int64_t sbp_cnn_param_count(const sbp_cnn* net);
+sbp_status sbp_cnn_get_params(sbp_cnn* net, float* host_params);
+/* Also resets the optimiser state. */
+sbp_status sbp_cnn_set_params(sbp_cnn* net, const float* host_params);
+sbp_status sbp_cnn_set_normalisation(sbp_cnn* net, const float* in_mean4, const float* in_scale4,
+                                     const float* out_scale4);
+/* Forward pass of n images (dtype SBP_F32 or SBP_F64 state); sbp_cnn_output copies y
+ * ([n][64*64][8] FP32, channels 0..3 used) to a device buffer. */
+sbp_status sbp_cnn_forward(sbp_cnn* net, int n, const void* d_coarse, int dtype, int64_t img_stride);
+sbp_status sbp_cnn_output(sbp_cnn* net, int n, float* d_y);
+/* Forward and backward; loss (optional, synchronises) and the gradient of every parameter
+ * (optional host copy, sbp_cnn_param_count floats).  d_fine_r: [n][4][64][64] FP64. */
+sbp_status sbp_cnn_gradients(sbp_cnn* net, int n, const void* d_coarse, int dtype, int64_t img_stride,
+                             const double* d_fine_r, float* loss, float* host_grads);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the gradients of this batch. */
+sbp_status sbp_cnn_train_step(sbp_cnn* net, int n, const void* d_coarse, int dtype, int64_t img_stride,
+                              const double* d_fine_r, float lr, float* loss);
+/* corrected = coarse + y * out_scale, FP64 [n][4][64][64] into d_out. */
+sbp_status sbp_cnn_apply(sbp_cnn* net, int n, const void* d_coarse, int dtype, int64_t img_stride, double* d_out);
+/* Restriction of n fine images [n][4][nf][nf] (FP64, on linspace nodes) to [n][4][nc][nc] by
+ * tensor-product 6-point Lagrange interpolation at the coarse linspace nodes (exact for
+ * polynomials of degree 5 in each direction; one-sided stencils at the ends). */
+sbp_status sbp_restrict_linspace(int n, int nf, int nc, const double* d_fine, double* d_coarse, void* stream);
+/* Per image relative L2 difference |a - b| / |b| over 4 planes of `points` points each. */
+sbp_status sbp_rel_l2_images(int n, int64_t points, const void* d_a, int dtype_a, int64_t stride_a,
+                             const void* d_b, int dtype_b, int64_t stride_b, double* d_out, void* stream);
 
 #ifdef __cplusplus
 }

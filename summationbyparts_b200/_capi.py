@@ -67,6 +67,7 @@ SIGNATURES = {
     "sbp_system_get_state": (_i, [_vp, _i, _dp]),
     "sbp_system_set_state_all": (_i, [_vp, _i, _vp]),
     "sbp_system_get_state_all": (_i, [_vp, _i, _vp]),
+    "sbp_system_get_state_all_device": (_i, [_vp, _i, _vp]),
     "sbp_system_state_count": (_i64, [_vp, _i]),
     "sbp_system_set_dt": (_i, [_vp, _i, _d]),
     "sbp_system_set_time": (_i, [_vp, _i, _d]),
@@ -84,6 +85,21 @@ SIGNATURES = {
     "sbp_system_group_count": (_i, [_vp]),
     "sbp_system_group_info": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i64)]),
     "sbp_system_launch_stage": (_i, [_vp, _i, _i, _i]),
+    "sbp_cnn_create": (_i, [_i, _i, ctypes.c_ulonglong, ctypes.POINTER(_vp)]),
+    "sbp_cnn_destroy": (_i, [_vp]),
+    "sbp_cnn_set_stream": (_i, [_vp, _vp]),
+    "sbp_cnn_synchronize": (_i, [_vp]),
+    "sbp_cnn_param_count": (_i64, [_vp]),
+    "sbp_cnn_get_params": (_i, [_vp, _vp]),
+    "sbp_cnn_set_params": (_i, [_vp, _vp]),
+    "sbp_cnn_set_normalisation": (_i, [_vp, _vp, _vp, _vp]),
+    "sbp_cnn_forward": (_i, [_vp, _i, _vp, _i, _i64]),
+    "sbp_cnn_output": (_i, [_vp, _i, _vp]),
+    "sbp_cnn_gradients": (_i, [_vp, _i, _vp, _i, _i64, _vp, ctypes.POINTER(ctypes.c_float), _vp]),
+    "sbp_cnn_train_step": (_i, [_vp, _i, _vp, _i, _i64, _vp, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+    "sbp_cnn_apply": (_i, [_vp, _i, _vp, _i, _i64, _vp]),
+    "sbp_restrict_linspace": (_i, [_i, _i, _i, _vp, _vp, _vp]),
+    "sbp_rel_l2_images": (_i, [_i, _i64, _vp, _i, _i64, _vp, _i, _i64, _vp, _vp]),
 }
 
 

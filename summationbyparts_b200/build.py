@@ -34,6 +34,7 @@ UNITS = {
     "system_kernels.cu": EXACT,
     "op_apply.cu": EXACT,
     "metrics_noalloc.cu": EXACT,
+    "cnn.cu": [],
     "stage_f64_u4.cu": EXACT,
     "stage_f64_u9.cu": EXACT,
     "stage_f64_sbp.cu": EXACT,

@@ -793,6 +793,17 @@ sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q) {
     return SBP_OK;
 }
 
+sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q) {
+    clear_error();
+    if (!sys || !d_q || (dtype != SBP_F64 && dtype != SBP_F32)) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    cudaStream_t st = sys->st();
+    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+                            dtype, sys->prev_hi, sys->prev_lo, d_q, sys->max_points, st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    return SBP_OK;
+}
+
 sbp_status sbp_system_set_dt(sbp_system* sys, int instance, double dt) {
     clear_error();
     if (!sys || instance >= sys->ninst) return SBP_ERR_INVALID_ARGUMENT;

@@ -177,6 +177,10 @@ class BlockSystem:
         ptr = buf.ctypes.data if isinstance(buf, np.ndarray) else buf.data_ptr()
         check(_capi.lib.sbp_system_get_state_all(self.h, dtype, ctypes.c_void_p(ptr)))
 
+    def get_state_all_device(self, d_ptr: int, dtype: int = F64) -> None:
+        """Pack every block's state into device memory at d_ptr (state_count(dtype) elements)."""
+        check(_capi.lib.sbp_system_get_state_all_device(self.h, dtype, ctypes.c_void_p(d_ptr)))
+
     # -- stepping and diagnostics
     def max_dt(self, instance: int = 0) -> float:
         dt = ctypes.c_double()
