@@ -58,8 +58,25 @@ typedef enum sbp_dtype { SBP_F64 = 0, SBP_F32 = 1 } sbp_dtype;
  * a compensated (hi, lo) f32 pair; metrics built in f64, SAT terms and norms in f64. */
 typedef enum sbp_precision { SBP_PRECISION_F64 = 0, SBP_PRECISION_F32_COMPENSATED = 1 } sbp_precision;
 
-/* euler::BoundaryCharacteristic (euler/src/lib.rs:737-745): This, Grid(neighbour), Vortex. */
-typedef enum sbp_boundary_kind { SBP_BC_THIS = 0, SBP_BC_GRID = 1, SBP_BC_VORTEX = 2 } sbp_boundary_kind;
+/* euler::BoundaryCharacteristic (euler/src/lib.rs:737-745): This, Grid(neighbour), Vortex,
+ * Interpolate(neighbour, operator) (a 2:1 interface) and MultiGrid(segments). */
+typedef enum sbp_boundary_kind {
+    SBP_BC_THIS = 0,
+    SBP_BC_GRID = 1,
+    SBP_BC_VORTEX = 2,
+    SBP_BC_INTERPOLATE = 3,
+    SBP_BC_MULTIGRID = 4
+} sbp_boundary_kind;
+
+/* sbp::operators::{Interpolation4, Interpolation8, Interpolation9, Interpolation9h2}
+ * (sbp/src/operators/interpolation/*.rs).  Fine lines have 2 n - 1 points for a coarse line of
+ * n points (2 (n - 1) for Interpolation9h2). */
+typedef enum sbp_interpolation {
+    SBP_INTERP4 = 0,
+    SBP_INTERP8 = 1,
+    SBP_INTERP9 = 2,
+    SBP_INTERP9H2 = 3
+} sbp_interpolation;
 
 enum { SBP_NORTH = 0, SBP_SOUTH = 1, SBP_EAST = 2, SBP_WEST = 3 };
 
@@ -80,8 +97,13 @@ typedef struct sbp_block_desc {
     const double* x;      /* host, (ny, nx) */
     const double* y;      /* host, (ny, nx) */
     int bc_kind[4];       /* sbp_boundary_kind per direction */
-    int bc_neighbour[4];  /* block index for SBP_BC_GRID */
+    int bc_neighbour[4];  /* block index for SBP_BC_GRID and SBP_BC_INTERPOLATE */
     int instance;         /* 0 .. ninstances-1 */
+    int bc_interp_op[4];  /* SBP_BC_INTERPOLATE: sbp_interpolation; fine2coarse when this block's
+                             nx is smaller than the neighbour's (euler/src/lib.rs:818) */
+    int bc_multigrid_count[4];   /* SBP_BC_MULTIGRID: number of segments */
+    const int* bc_multigrid[4];  /* SBP_BC_MULTIGRID: (block, start, end) per segment, host
+                                    memory read at creation (euler/src/lib.rs:829-846) */
 } sbp_block_desc;
 
 typedef struct sbp_system sbp_system;
@@ -121,6 +143,12 @@ sbp_status sbp_dissxi(int op, int dtype, const void* d_prev, void* d_fut, int64_
 /* UpwindOperator2d::disseta (sbp/src/operators.rs:98-100). */
 sbp_status sbp_disseta(int op, int dtype, const void* d_prev, void* d_fut, int64_t ny, int64_t nx,
                        int64_t nbatch, int64_t batch_stride, void* stream);
+/* InterpolationOperator::fine2coarse / coarse2fine (sbp/src/operators.rs:108-113) of nbatch
+ * lines: line b of d_in starts at b * in_stride, of d_out at b * out_stride.  fine2coarse != 0:
+ * n_in fine points -> n_out coarse points; else coarse -> fine.  The sizes must satisfy the
+ * operator's relation.  Bit-identical to the reference's unfused sums in the same dtype. */
+sbp_status sbp_interpolate(int op, int fine2coarse, int dtype, const void* d_in, void* d_out, int64_t n_in,
+                           int64_t n_out, int64_t nbatch, int64_t in_stride, int64_t out_stride, void* stream);
 
 /* Grid::metrics / Metrics::new (sbp/src/grid.rs:64-140) in f64 on device:
  * d_metrics receives 5 planes (detj, detj*dxi/dx, detj*dxi/dy, detj*deta/dx, detj*deta/dy).

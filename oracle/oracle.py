@@ -22,7 +22,8 @@ OPERATORS = {"upwind4": UPWIND4, "upwind4h2": UPWIND4H2, "upwind9": UPWIND9,
 DIFF, DISS = 0, 1
 XI, ETA = 0, 1
 F64, F32 = 0, 1
-BC_THIS, BC_GRID, BC_VORTEX = 0, 1, 2
+BC_THIS, BC_GRID, BC_VORTEX, BC_INTERPOLATE, BC_MULTIGRID = 0, 1, 2, 3, 4
+INTERP4, INTERP8, INTERP9, INTERP9H2 = 0, 1, 2, 3
 NORTH, SOUTH, EAST, WEST = 0, 1, 2, 3
 
 
@@ -34,7 +35,9 @@ class VortexParams(ctypes.Structure):
 class BlockDesc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("op_xi", ctypes.c_int), ("op_eta", ctypes.c_int),
                 ("x", ctypes.POINTER(ctypes.c_double)), ("y", ctypes.POINTER(ctypes.c_double)),
-                ("bc_kind", ctypes.c_int * 4), ("bc_neighbour", ctypes.c_int * 4)]
+                ("bc_kind", ctypes.c_int * 4), ("bc_neighbour", ctypes.c_int * 4),
+                ("bc_interp_op", ctypes.c_int * 4), ("bc_mg_count", ctypes.c_int * 4),
+                ("bc_mg", ctypes.POINTER(ctypes.c_int) * 4)]
 
 
 def build() -> None:
@@ -76,6 +79,8 @@ def lib(fast: bool = False) -> ctypes.CDLL:
                           ctypes.c_int64, ctypes.c_int64, ctypes.c_int, dp]
     L.orc_h2_err.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int64, ctypes.c_int64]
     L.orc_h2_err.restype = ctypes.c_double
+    L.orc_interpolate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_void_p, ctypes.c_int64]
     L.orc_system_create.argtypes = [ctypes.POINTER(BlockDesc), ctypes.c_int, ctypes.c_double]
     L.orc_system_create.restype = ctypes.c_void_p
     L.orc_system_destroy.argtypes = [ctypes.c_void_p]
@@ -189,6 +194,41 @@ def h2_err(op_xi, op_eta, a, b) -> float:
     return lib().orc_h2_err(op_xi, op_eta, _dp(np.ascontiguousarray(a)), _dp(np.ascontiguousarray(b)), ny, nx)
 
 
+def set_bc(desc, d, bc, keep):
+    """bc: (kind, neighbour), (BC_INTERPOLATE, neighbour, operator) or
+    (BC_MULTIGRID, [(grid, start, end), ...])."""
+    kind = bc[0]
+    desc.bc_kind[d] = kind
+    desc.bc_neighbour[d] = 0
+    if kind == BC_MULTIGRID:
+        tri = np.ascontiguousarray(np.array(bc[1], dtype=np.int32).reshape(-1))
+        keep.append(tri)
+        desc.bc_mg_count[d] = tri.size // 3
+        desc.bc_mg[d] = tri.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    else:
+        desc.bc_neighbour[d] = bc[1]
+        if kind == BC_INTERPOLATE:
+            desc.bc_interp_op[d] = bc[2]
+
+
+def interpolate(op: int, fine2coarse: bool, x, dtype=np.float64) -> np.ndarray:
+    """InterpolationOperator::fine2coarse / coarse2fine of one line (f64, or the reference's f32
+    build for dtype float32)."""
+    x = np.ascontiguousarray(x, dtype=dtype)
+    n = x.size
+    odd = op != INTERP9H2
+    if fine2coarse:
+        m = (n + 1) // 2 if odd else n // 2 + 1
+    else:
+        m = 2 * n - 1 if odd else 2 * (n - 1)
+    out = np.empty(m, dtype=dtype)
+    L = lib(False)
+    dt = F64 if x.dtype == np.float64 else F32
+    if L.orc_interpolate(op, int(fine2coarse), dt, x.ctypes.data, n, out.ctypes.data, m) != 0:
+        raise ValueError("orc_interpolate: bad operator or sizes")
+    return out
+
+
 class System:
     """Multi-block system with the reference's single-threaded multigrid semantics."""
 
@@ -205,7 +245,7 @@ class System:
             arr[i].op_xi, arr[i].op_eta = b["op_xi"], b["op_eta"]
             arr[i].x, arr[i].y = _dp(x), _dp(y)
             for d in range(4):
-                arr[i].bc_kind[d], arr[i].bc_neighbour[d] = b["bc"][d]
+                set_bc(arr[i], d, b["bc"][d], self._keep)
         self.shapes = [(int(arr[i].ny), int(arr[i].nx)) for i in range(len(blocks))]
         self.h = self._L.orc_system_create(arr, len(blocks), gamma)
         if not self.h:

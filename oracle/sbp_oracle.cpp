@@ -9,6 +9,7 @@
  */
 #include "sbp_oracle.h"
 #include "oracle_coefficients.h"
+#include "oracle_interp_coefficients.h"
 
 #include <algorithm>
 #include <atomic>
@@ -585,6 +586,7 @@ static double h2_err(int opx, int ope, const double* a, const double* b, int64_t
 /* ------------------------------------------------------------------------- */
 
 struct orc_system {
+    std::vector<std::vector<int>> mg[4];  // copies of the MultiGrid triples per block and side
     double gamma = 1.4;
     double time = 0.0;
     std::vector<orc_block_desc> desc;
@@ -599,6 +601,71 @@ struct orc_system {
 };
 
 namespace {
+
+/* Interpolation operator tables (oracle_interp_coefficients.h, transcribed from the reference:
+ * f64 values and the reference's f32-build values). */
+template <class T>
+struct InterpTable {
+    int brows, bcols, drows, dcols, jump0, jump1;
+    const T* block;
+    const T* diag;
+};
+#define ORC_INTERP_TABLES(P)                                                                                   \
+    static const double kI##P##_F2C_B[] = {ORCI_##P##_F2C_BLOCK}, kI##P##_F2C_D[] = {ORCI_##P##_F2C_DIAG};     \
+    static const double kI##P##_C2F_B[] = {ORCI_##P##_C2F_BLOCK}, kI##P##_C2F_D[] = {ORCI_##P##_C2F_DIAG};     \
+    static const float kJ##P##_F2C_B[] = {ORCI_##P##_F2C_BLOCK_F32}, kJ##P##_F2C_D[] = {ORCI_##P##_F2C_DIAG_F32}; \
+    static const float kJ##P##_C2F_B[] = {ORCI_##P##_C2F_BLOCK_F32}, kJ##P##_C2F_D[] = {ORCI_##P##_C2F_DIAG_F32};
+ORC_INTERP_TABLES(4)
+ORC_INTERP_TABLES(8)
+ORC_INTERP_TABLES(9)
+ORC_INTERP_TABLES(9H2)
+#undef ORC_INTERP_TABLES
+#define ORC_INTERP_ENTRY(T, K, P, D)                                                                           \
+    InterpTable<T> {                                                                                           \
+        ORCI_##P##_##D##_BROWS, ORCI_##P##_##D##_BCOLS, ORCI_##P##_##D##_DROWS, ORCI_##P##_##D##_DCOLS,       \
+            ORCI_##P##_##D##_JUMP0, ORCI_##P##_##D##_JUMP1, K##P##_##D##_B, K##P##_##D##_D                    \
+    }
+#define ORC_INTERP_ROWS(T, K)                                                                                  \
+    {{ORC_INTERP_ENTRY(T, K, 4, C2F), ORC_INTERP_ENTRY(T, K, 4, F2C)},                                         \
+     {ORC_INTERP_ENTRY(T, K, 8, C2F), ORC_INTERP_ENTRY(T, K, 8, F2C)},                                         \
+     {ORC_INTERP_ENTRY(T, K, 9, C2F), ORC_INTERP_ENTRY(T, K, 9, F2C)},                                         \
+     {ORC_INTERP_ENTRY(T, K, 9H2, C2F), ORC_INTERP_ENTRY(T, K, 9H2, F2C)}}
+static const InterpTable<double> kInterp[4][2] = ORC_INTERP_ROWS(double, kI);
+static const InterpTable<float> kInterp32[4][2] = ORC_INTERP_ROWS(float, kJ);
+#undef ORC_INTERP_ROWS
+#undef ORC_INTERP_ENTRY
+static const bool kInterpFineOdd[4] = {ORCI_4_FINE_ODD != 0, ORCI_8_FINE_ODD != 0, ORCI_9_FINE_ODD != 0,
+                                       ORCI_9H2_FINE_ODD != 0};
+
+/* interpolate (sbp/src/operators/interpolation.rs:15-50): every output starts at 0 and
+ * accumulates out += in * c over all columns of its row (zeros included), unfused, in T. */
+template <class T>
+static void interpolate(const T* in, int64_t nin, T* out, int64_t nout, const InterpTable<T>& I) {
+    for (int64_t i = 0; i < nout; ++i) {
+        T t = T(0);
+        if (i < I.brows) {
+            for (int k = 0; k < I.bcols; ++k) t = t + in[k] * I.block[i * I.bcols + k];
+        } else if (nout - i <= I.brows) {
+            const int64_t row = nout - i - 1;
+            const int64_t index = nin - I.bcols;
+            for (int k = 0; k < I.bcols; ++k) {
+                const int col = I.bcols - k - 1;
+                t = t + in[index + k] * I.block[row * I.bcols + col];
+            }
+        } else {
+            const int64_t n = i - I.brows;
+            const int64_t index = I.jump0 + I.jump1 * (n / I.drows);
+            const int64_t row = n % I.drows;
+            for (int k = 0; k < I.dcols; ++k) t = t + in[index + k] * I.diag[row * I.dcols + k];
+        }
+        out[i] = t;
+    }
+}
+
+/* the size relation the operator asserts (fine = 2 coarse - 1, or 2 (coarse - 1) for 9h2) */
+static bool interp_sizes_ok(int op, int64_t fine, int64_t coarse) {
+    return kInterpFineOdd[op] ? fine == 2 * coarse - 1 : fine == 2 * (coarse - 1);
+}
 
 /* Edge extraction of a field: north = last row, south = row 0, east = last column, west = column 0. */
 static void edge_of(const std::vector<double>& q, int64_t ny, int64_t nx, int d, std::vector<double>& out) {
@@ -637,6 +704,49 @@ static int extract(orc_system* s, const std::vector<std::vector<double>>& fields
             edge_of(fields[g], G.ny, G.nx, opposite(d), buf);
             const int64_t len = (d == ORC_NORTH || d == ORC_SOUTH) ? D.nx : D.ny;
             if ((int64_t)buf.size() != 4 * len) return -3;
+        } else if (kind == ORC_BC_INTERPOLATE) {
+            // euler/src/lib.rs:816-827: fine2coarse when this block's nx is the smaller one
+            const int g = D.bc_neighbour[d];
+            const int op = D.bc_interp_op[d];
+            if (op < 0 || op > 3) return -1;
+            const orc_block_desc& G = s->desc[g];
+            std::vector<double> from;
+            edge_of(fields[g], G.ny, G.nx, opposite(d), from);
+            const bool f2c = D.nx < G.nx;
+            const int64_t len = (d == ORC_NORTH || d == ORC_SOUTH) ? D.nx : D.ny;
+            const int64_t lg = (int64_t)from.size() / 4;
+            if (f2c ? !interp_sizes_ok(op, lg, len) : !interp_sizes_ok(op, len, lg)) return -3;
+            buf.assign(4 * len, 0.0);
+            for (int c = 0; c < 4; ++c) interpolate(from.data() + c * lg, lg, buf.data() + c * len, len, kInterp[op][f2c]);
+        } else if (kind == ORC_BC_MULTIGRID) {
+            // euler/src/lib.rs:829-846, as written: each segment (g, start, end) of the
+            // neighbours' opposite edges is copied in turn, the next one starting on the last
+            // point of the previous; the first point of every segment but the last is halved.
+            const int64_t len = (d == ORC_NORTH || d == ORC_SOUTH) ? D.nx : D.ny;
+            const std::vector<int>& mg = s->mg[d][b];
+            buf.assign(4 * len, 0.0);
+            int64_t i = 0;
+            int remaining = (int)mg.size() / 3;
+            if (remaining == 0) return -3;
+            for (size_t sgi = 0; sgi + 2 < mg.size(); sgi += 3) {
+                const int g = mg[sgi], start = mg[sgi + 1], end = mg[sgi + 2];
+                const orc_block_desc& G = s->desc[g];
+                std::vector<double> from;
+                edge_of(fields[g], G.ny, G.nx, opposite(d), from);
+                const int64_t lg = (int64_t)from.size() / 4;
+                const int64_t n = end - start;
+                if (start < 0 || end > lg || n <= 0 || i + n > len) return -3;
+                for (int c = 0; c < 4; ++c)
+                    for (int64_t j = 0; j < n; ++j) buf[c * len + i + j] = from[c * lg + start + j];
+                remaining -= 1;
+                if (remaining == 0) {
+                    i += n;
+                    if (i != len) return -3;
+                } else {
+                    for (int c = 0; c < 4; ++c) buf[c * len + i] /= 2.0;
+                    i += n - 1;
+                }
+            }
         } else if (kind == ORC_BC_VORTEX) {
             const bool ns = d == ORC_NORTH || d == ORC_SOUTH;
             const int64_t len = ns ? D.nx : D.ny;
@@ -789,10 +899,29 @@ double orc_h2_err(int op_xi, int op_eta, const double* a, const double* b, int64
     return h2_err(op_xi, op_eta, a, b, ny, nx);
 }
 
+int orc_interpolate(int op, int fine2coarse, int dtype, const void* in, int64_t n_in, void* out, int64_t n_out) {
+    if (op < 0 || op > 3 || !in || !out || (dtype != ORC_F64 && dtype != ORC_F32)) return -1;
+    const bool f2c = fine2coarse != 0;
+    if (f2c ? !interp_sizes_ok(op, n_in, n_out) : !interp_sizes_ok(op, n_out, n_in)) return -1;
+    if (dtype == ORC_F64)
+        interpolate(static_cast<const double*>(in), n_in, static_cast<double*>(out), n_out, kInterp[op][f2c]);
+    else
+        interpolate(static_cast<const float*>(in), n_in, static_cast<float*>(out), n_out, kInterp32[op][f2c]);
+    return 0;
+}
+
 orc_system* orc_system_create(const orc_block_desc* blocks, int nblocks, double gamma) {
     orc_system* s = new orc_system();
     s->gamma = gamma;
     s->desc.assign(blocks, blocks + nblocks);
+    for (int d = 0; d < 4; ++d) {
+        s->mg[d].resize(nblocks);
+        for (int b = 0; b < nblocks; ++b) {
+            if (blocks[b].bc_kind[d] == ORC_BC_MULTIGRID && blocks[b].bc_mg[d] && blocks[b].bc_mg_count[d] > 0)
+                s->mg[d][b].assign(blocks[b].bc_mg[d], blocks[b].bc_mg[d] + 3 * blocks[b].bc_mg_count[d]);
+            s->desc[b].bc_mg[d] = nullptr;
+        }
+    }
     s->x.resize(nblocks);
     s->y.resize(nblocks);
     s->metrics.resize(nblocks);

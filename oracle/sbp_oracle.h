@@ -34,7 +34,9 @@ enum { ORC_UPWIND4 = 0, ORC_UPWIND4H2 = 1, ORC_UPWIND9 = 2, ORC_UPWIND9H2 = 3, O
 enum { ORC_DIFF = 0, ORC_DISS = 1 };
 enum { ORC_XI = 0, ORC_ETA = 1 };
 enum { ORC_F64 = 0, ORC_F32 = 1 };
-enum { ORC_BC_THIS = 0, ORC_BC_GRID = 1, ORC_BC_VORTEX = 2 };
+enum { ORC_BC_THIS = 0, ORC_BC_GRID = 1, ORC_BC_VORTEX = 2, ORC_BC_INTERPOLATE = 3, ORC_BC_MULTIGRID = 4 };
+/* interpolation operators (sbp/src/operators/interpolation*.rs) */
+enum { ORC_INTERP4 = 0, ORC_INTERP8 = 1, ORC_INTERP9 = 2, ORC_INTERP9H2 = 3 };
 enum { ORC_NORTH = 0, ORC_SOUTH = 1, ORC_EAST = 2, ORC_WEST = 3 };
 
 typedef struct {
@@ -50,6 +52,9 @@ typedef struct {
     const double* y; /* (ny, nx) */
     int bc_kind[4];  /* ORC_BC_* per direction N, S, E, W */
     int bc_neighbour[4];
+    int bc_interp_op[4];   /* ORC_BC_INTERPOLATE: ORC_INTERP* */
+    int bc_mg_count[4];    /* ORC_BC_MULTIGRID: number of (grid, start, end) triples */
+    const int* bc_mg[4];   /* ORC_BC_MULTIGRID: the triples (copied at creation) */
 } orc_block_desc;
 
 typedef struct orc_system orc_system;
@@ -74,6 +79,11 @@ int orc_vortex(const orc_vortex_params* vp, double gamma, double t, const double
 int orc_rhs(int op_xi, int op_eta, double gamma, const double* q, const double* metrics,
             const double* zn, const double* zs, const double* ze, const double* zw,
             int64_t ny, int64_t nx, int force_trad, double* k);
+
+/* InterpolationOperator::fine2coarse / coarse2fine (sbp/src/operators/interpolation.rs:15-50 and
+ * interpolation{4,8,9,9h2}.rs) of one line.  Returns -1 for an unknown operator or sizes that
+ * break the operator's assert (fine = 2 coarse - 1, or 2 (coarse - 1) for 9h2). */
+int orc_interpolate(int op, int fine2coarse, int dtype, const void* in, int64_t n_in, void* out, int64_t n_out);
 
 /* Field::h2_err (euler/src/lib.rs:377-431) */
 double orc_h2_err(int op_xi, int op_eta, const double* a, const double* b, int64_t ny, int64_t nx);

@@ -18,7 +18,8 @@ STATUS_NAMES = {0: "SBP_OK", 1: "SBP_ERR_INVALID_ARGUMENT", 2: "SBP_ERR_SHAPE", 
 
 F64, F32 = 0, 1
 PRECISION_F64, PRECISION_F32_COMPENSATED = 0, 1
-BC_THIS, BC_GRID, BC_VORTEX = 0, 1, 2
+BC_THIS, BC_GRID, BC_VORTEX, BC_INTERPOLATE, BC_MULTIGRID = 0, 1, 2, 3, 4
+INTERP4, INTERP8, INTERP9, INTERP9H2 = 0, 1, 2, 3
 NORTH, SOUTH, EAST, WEST = 0, 1, 2, 3
 
 
@@ -38,7 +39,9 @@ class VortexParams(ctypes.Structure):
 class BlockDesc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("op_xi", ctypes.c_int), ("op_eta", ctypes.c_int),
                 ("x", ctypes.POINTER(ctypes.c_double)), ("y", ctypes.POINTER(ctypes.c_double)),
-                ("bc_kind", ctypes.c_int * 4), ("bc_neighbour", ctypes.c_int * 4), ("instance", ctypes.c_int)]
+                ("bc_kind", ctypes.c_int * 4), ("bc_neighbour", ctypes.c_int * 4), ("instance", ctypes.c_int),
+                ("bc_interp_op", ctypes.c_int * 4), ("bc_multigrid_count", ctypes.c_int * 4),
+                ("bc_multigrid", ctypes.POINTER(ctypes.c_int) * 4)]
 
 
 _i, _i64, _d, _vp = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
@@ -55,6 +58,7 @@ SIGNATURES = {
     "sbp_diffxi": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "sbp_diffeta": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "sbp_dissxi": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
+    "sbp_interpolate": (_i, [_i, _i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
     "sbp_disseta": (_i, [_i, _i, _vp, _vp, _i64, _i64, _i64, _i64, _vp]),
     "sbp_metrics": (_i, [_i, _i, _vp, _vp, _i64, _i64, _vp, _vp]),
     "sbp_metrics_noalloc": (_i, [_i, _i, _vp, _vp, _i64, _i64, _vp, _vp]),

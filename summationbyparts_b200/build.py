@@ -35,6 +35,7 @@ UNITS = {
     "op_apply.cu": EXACT,
     "metrics_noalloc.cu": EXACT,
     "cnn.cu": [],
+    "interp.cu": EXACT,
     "stage_f64_u4.cu": EXACT,
     "stage_f64_u9.cu": EXACT,
     "stage_f64_sbp.cu": EXACT,

@@ -13,7 +13,7 @@
 
 namespace sbp {
 
-enum { BC_THIS = 0, BC_GRID = 1, BC_VORTEX = 2 };
+enum { BC_THIS = 0, BC_GRID = 1, BC_VORTEX = 2, BC_INTERPOLATE = 3, BC_MULTIGRID = 4 };
 enum { NORTH = 0, SOUTH = 1, EAST = 2, WEST = 3 };
 enum : unsigned { STATUS_RHO = 1u, STATUS_P = 2u, STATUS_DETJ = 4u, STATUS_NAN = 8u };
 
@@ -25,6 +25,8 @@ struct BlockDev {
     int simd_f32;  // same for f32x16 lanes
     int bc_kind[4];
     int bc_nb[4];
+    int bc_aux[4];   // BC_INTERPOLATE: interpolation operator; BC_MULTIGRID: first segment in the table
+    int bc_aux2[4];  // BC_MULTIGRID: number of segments
     int64_t q_off, m_off, x_off;
     int64_t e_off;  // slot of this block's first edge point in the edge-k buffer (see edge_index)
     double idx_xi, idx_eta;  // 1/(1/(n-1)) per direction, f64

@@ -37,6 +37,7 @@
 #include <type_traits>
 
 #include "euler_device.cuh"
+#include "interp.cuh"
 #include "sbp_ops.cuh"
 
 namespace sbp {
@@ -61,6 +62,7 @@ struct StageArgs {
     T* new_hi;               // new state (stage 3)
     T* new_lo;
     T* kedge;                // k of block-edge points, 4 per point (edge_index order per block)
+    const int4* mg;          // MultiGrid segments (block, start, end, -) of all block sides
     const T* met;            // metric planes in T
     const double* met64;     // metric planes in f64 (SAT terms)
     const double* xy;        // coordinates
@@ -484,6 +486,15 @@ __device__ __forceinline__ void rk_update(const StageArgs<T>& A, int64_t e, T qv
     }
 }
 
+// Element of a block's edge opposite to side d (north -> the block's south row, ...) at position
+// k along that edge: the point whose state a neighbour's side-d SAT reads.
+__device__ __forceinline__ int opposite_edge_point(int d, int k, int gnx, int gny) {
+    if (d == NORTH) return k;                      // south row
+    if (d == SOUTH) return (gny - 1) * gnx + k;    // north row
+    if (d == EAST) return k * gnx;                 // west column
+    return k * gnx + (gnx - 1);                    // east column
+}
+
 // SATs of one block-edge point in the reference's order N, S, E, W; k updated in place.
 template <class T>
 __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int row,
@@ -501,16 +512,56 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         if (kind == BC_VORTEX) {
             const double* xy = A.xy + B.x_off;
             vortex_point(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+        } else if (kind == BC_INTERPOLATE || kind == BC_MULTIGRID) {
+            // boundary_extract (euler/src/lib.rs:816-846): data from neighbours' opposite edges
+            const bool ns_ = d == NORTH || d == SOUTH;
+            const int i = ns_ ? col : row;       // position along this edge
+            const int len = ns_ ? nx : ny;
+            if (kind == BC_INTERPOLATE) {
+                const BlockDev& Gb = A.blocks[B.bc_nb[d]];
+                const T* gq = A.u_in + Gb.q_off;
+                const int lg = ns_ ? Gb.nx : Gb.ny;
+                const bool f2c = nx < Gb.nx;  // fine2coarse when this block's nx is smaller (:818)
+                // in f64 for both state precisions (the f32 state widened), as the SAT itself
+                const InterpDev<double> ip = interp_dev<double>(B.bc_aux[d], f2c);
+#pragma unroll 1
+                for (int cc = 0; cc < 4; ++cc) {
+                    const T* plane = gq + cc * (int64_t)Gb.npad;
+                    zv[cc] = interp_at<double>(ip, i, lg, len, [&](int64_t k) {
+                        return double(plane[opposite_edge_point(d, (int)k, Gb.nx, Gb.ny)]);
+                    });
+                }
+            } else {
+                // Segments (g, start, end) are laid end to end, each starting on the previous
+                // one's last point; the first point of every segment but the last is halved.
+                const int4* sg = A.mg + B.bc_aux[d];
+                const int nseg = B.bc_aux2[d];
+                int p0 = 0, hit = 0, hp = 0;
+                for (int k = 0; k < nseg; ++k) {
+                    const int n = sg[k].z - sg[k].y;
+                    if (i >= p0 && i < p0 + n) {
+                        hit = k;
+                        hp = p0;
+                    }
+                    p0 += n - 1;
+                }
+                const int4 seg = sg[hit];
+                const BlockDev& Gb = A.blocks[seg.x];
+                const T* gq = A.u_in + Gb.q_off;
+                const int gp = opposite_edge_point(d, seg.y + (i - hp), Gb.nx, Gb.ny);
+                const bool halve = i == hp && hit != nseg - 1;
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    const double v = double(gq[cc * (int64_t)Gb.npad + gp]);
+                    zv[cc] = halve ? v / 2.0 : v;
+                }
+            }
         } else {
             // This: own opposite edge; Grid(g): neighbour's opposite edge
             // (boundary_extracts, euler/src/lib.rs:869-930).
             const BlockDev& Gb = kind == BC_GRID ? A.blocks[B.bc_nb[d]] : B;
             const T* gq = A.u_in + Gb.q_off;
-            int gp;
-            if (d == NORTH) gp = col;                             // g.south
-            else if (d == SOUTH) gp = (Gb.ny - 1) * Gb.nx + col;  // g.north
-            else if (d == EAST) gp = row * Gb.nx;                 // g.west
-            else gp = row * Gb.nx + (Gb.nx - 1);                  // g.east
+            const int gp = opposite_edge_point(d, (d == NORTH || d == SOUTH) ? col : row, Gb.nx, Gb.ny);
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc) zv[cc] = double(gq[cc * (int64_t)Gb.npad + gp]);
         }

@@ -16,6 +16,7 @@
 
 #include "common.h"
 #include "euler_device.cuh"
+#include "interp.cuh"
 #include "op_apply.h"
 #include "sbp_ops.cuh"
 #include "stage_dispatch.h"
@@ -117,6 +118,7 @@ struct sbp_system {
     void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
     int64_t nedge = 0;
+    int4* d_mg = nullptr;    // MultiGrid segments of all block sides
     // schedule
     int TY = 16, TX = kTileX, threads = kStageThreads;
     std::vector<int> active;
@@ -157,7 +159,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge};
+                    s->d_coef,   s->kedge,  s->d_mg};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -222,6 +224,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
     a.kedge = static_cast<T*>(s->kedge);
+    a.mg = s->d_mg;
     a.gamma = s->gamma;
     a.status = s->status;
     return a;
@@ -452,9 +455,60 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         }
         for (int d = 0; d < 4; ++d) {
             const int k = D.bc_kind[d];
-            if (k != SBP_BC_THIS && k != SBP_BC_GRID && k != SBP_BC_VORTEX) {
+            if (k != SBP_BC_THIS && k != SBP_BC_GRID && k != SBP_BC_VORTEX && k != SBP_BC_INTERPOLATE &&
+                k != SBP_BC_MULTIGRID) {
                 set_error("block %d: unknown boundary kind %d", b, k);
                 return SBP_ERR_INVALID_ARGUMENT;
+            }
+            const bool ns = d == SBP_NORTH || d == SBP_SOUTH;
+            const int64_t mine = ns ? D.nx : D.ny;
+            if (k == SBP_BC_INTERPOLATE) {
+                const int g = D.bc_neighbour[d];
+                const int op = D.bc_interp_op[d];
+                if (g < 0 || g >= nblocks || op < 0 || op > 3) {
+                    set_error("block %d: interpolation neighbour %d or operator %d out of range", b, g, op);
+                    return SBP_ERR_INVALID_ARGUMENT;
+                }
+                if (blocks[g].instance != D.instance) {
+                    set_error("block %d: neighbour %d belongs to another instance", b, g);
+                    return SBP_ERR_INVALID_ARGUMENT;
+                }
+                const int64_t theirs = ns ? blocks[g].nx : blocks[g].ny;
+                const bool f2c = D.nx < blocks[g].nx;  // euler/src/lib.rs:818
+                const bool sizes = f2c ? interp_sizes_ok(op, theirs, mine) : interp_sizes_ok(op, mine, theirs);
+                if (!sizes || !interp_reads_in_range(op, f2c, theirs, mine)) {
+                    set_error("block %d: %s interpolation from %lld to %lld points does not fit the operator", b,
+                              f2c ? "fine2coarse" : "coarse2fine", (long long)theirs, (long long)mine);
+                    return SBP_ERR_SHAPE;
+                }
+            }
+            if (k == SBP_BC_MULTIGRID) {
+                const int nseg = D.bc_multigrid_count[d];
+                if (nseg < 1 || !D.bc_multigrid[d]) {
+                    set_error("block %d: multigrid boundary without segments", b);
+                    return SBP_ERR_INVALID_ARGUMENT;
+                }
+                int64_t cover = 0;
+                for (int q = 0; q < nseg; ++q) {
+                    const int g = D.bc_multigrid[d][3 * q], st = D.bc_multigrid[d][3 * q + 1],
+                              en = D.bc_multigrid[d][3 * q + 2];
+                    if (g < 0 || g >= nblocks || blocks[g].instance != D.instance) {
+                        set_error("block %d: multigrid segment %d: bad block %d", b, q, g);
+                        return SBP_ERR_INVALID_ARGUMENT;
+                    }
+                    const int64_t theirs = ns ? blocks[g].nx : blocks[g].ny;
+                    if (st < 0 || en > theirs || en - st < 1) {
+                        set_error("block %d: multigrid segment %d [%d, %d) outside block %d's edge", b, q, st, en, g);
+                        return SBP_ERR_SHAPE;
+                    }
+                    cover += (en - st) - (q + 1 < nseg ? 1 : 0);
+                }
+                if (cover != mine) {
+                    // the reference asserts that the segments fill the edge (euler/src/lib.rs:840)
+                    set_error("block %d: multigrid segments cover %lld of %lld edge points", b, (long long)cover,
+                              (long long)mine);
+                    return SBP_ERR_SHAPE;
+                }
             }
             if (k == SBP_BC_GRID) {
                 const int g = D.bc_neighbour[d];
@@ -500,6 +554,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         if (e != cudaSuccess) return fail(cuda_status(e, "event"));
     }
     // layout
+    std::vector<int4> mg_host;
     s->hb.resize(nblocks);
     s->dense_off.resize(nblocks);
     s->hoff.resize(nblocks);
@@ -522,7 +577,15 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         B.simd_f32 = (int)(16 * (D.nx / 16));
         for (int d = 0; d < 4; ++d) {
             B.bc_kind[d] = D.bc_kind[d];
-            B.bc_nb[d] = D.bc_kind[d] == SBP_BC_GRID ? D.bc_neighbour[d] : b;
+            B.bc_nb[d] = (D.bc_kind[d] == SBP_BC_GRID || D.bc_kind[d] == SBP_BC_INTERPOLATE) ? D.bc_neighbour[d] : b;
+            if (D.bc_kind[d] == SBP_BC_INTERPOLATE) B.bc_aux[d] = D.bc_interp_op[d];
+            if (D.bc_kind[d] == SBP_BC_MULTIGRID) {
+                B.bc_aux[d] = (int)mg_host.size();
+                B.bc_aux2[d] = D.bc_multigrid_count[d];
+                for (int q = 0; q < D.bc_multigrid_count[d]; ++q)
+                    mg_host.push_back(make_int4(D.bc_multigrid[d][3 * q], D.bc_multigrid[d][3 * q + 1],
+                                                D.bc_multigrid[d][3 * q + 2], 0));
+            }
         }
         B.q_off = s->nq;
         B.m_off = s->nm;
@@ -583,6 +646,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
+    e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
     cudaStream_t st = s->stream;
     e = e ?: cudaMemsetAsync(s->prev_hi, 0, s->nq * ts, st);
@@ -597,6 +661,8 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: cudaMemcpyAsync(s->d_blocks, s->hb.data(), nblocks * sizeof(BlockDev), cudaMemcpyHostToDevice, st);
     e = e ?: cudaMemcpyAsync(s->d_inst, s->hi.data(), ninstances * sizeof(InstanceDev), cudaMemcpyHostToDevice, st);
     e = e ?: cudaMemcpyAsync(s->d_hoff, s->hoff.data(), nblocks * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    if (!mg_host.empty())
+        e = e ?: cudaMemcpyAsync(s->d_mg, mg_host.data(), mg_host.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
     std::vector<double> coef_host(12 * kCoefStride);  // large enough for either precision
     fill_coef_table(s->prec, coef_host.data(), kCoefStride, kCoefRow);
     e = e ?: cudaMemcpyAsync(s->d_coef, coef_host.data(), 12 * kCoefStride * ts, cudaMemcpyHostToDevice, st);

@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi
-from ._capi import BC_GRID, BC_THIS, BC_VORTEX, F32, F64, check  # noqa: F401
+from ._capi import BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX, F32, F64, check  # noqa: F401
 from .operators import SbpOperator2d
 
 PRECISIONS = {"f64": _capi.PRECISION_F64, "f32c": _capi.PRECISION_F32_COMPENSATED}
@@ -56,6 +56,23 @@ class BlockSpec:
     instance: int = 0
 
 
+def _set_bc(desc, d: int, bc) -> list:
+    """One side's boundary: (kind, neighbour) for This / Grid / Vortex, (BC_INTERPOLATE,
+    neighbour, operator) for a 2:1 interface, (BC_MULTIGRID, [(block, start, end), ...])."""
+    kind = bc[0]
+    desc.bc_kind[d] = kind
+    desc.bc_neighbour[d] = 0
+    if kind == BC_MULTIGRID:
+        tri = np.ascontiguousarray(np.array(bc[1], dtype=np.int32).reshape(-1))
+        desc.bc_multigrid_count[d] = tri.size // 3
+        desc.bc_multigrid[d] = tri.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        return [tri]
+    desc.bc_neighbour[d] = bc[1]
+    if kind == _capi.BC_INTERPOLATE:
+        desc.bc_interp_op[d] = bc[2]
+    return []
+
+
 class BlockSystem:
     def __init__(self, blocks: list[BlockSpec], ninstances: int = 1, precision: str = "f64", gamma: float = 1.4,
                  device: int = 0):
@@ -75,7 +92,7 @@ class BlockSystem:
             arr[i].x = x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             arr[i].y = y.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             for d in range(4):
-                arr[i].bc_kind[d], arr[i].bc_neighbour[d] = b.bc[d]
+                self._keep += _set_bc(arr[i], d, b.bc[d])
             arr[i].instance = b.instance
             self.shapes.append(x.shape)
         self.ninstances = ninstances

@@ -155,3 +155,17 @@ def test_multiblock_layout_is_conforming():
             assert other.bc[back] == (1, b)
     pts = sum(s.x.size for s in blocks)
     assert 30000 < pts < 40000
+
+
+def test_interpolate_rejects_bad_sizes():
+    """sbp_interpolate checks the operator's size relation and its read range before any device
+    work (so this runs without a GPU)."""
+    import ctypes
+    from summationbyparts_b200 import _capi
+    p = ctypes.c_void_p(16)
+    # fine must be 2 coarse - 1 (Interpolation9)
+    assert _capi.lib.sbp_interpolate(2, 1, _capi.F64, p, p, 40, 21, 1, 40, 21, None) == 2
+    # too short for the operator's boundary block (22 fine columns)
+    assert _capi.lib.sbp_interpolate(2, 1, _capi.F64, p, p, 21, 11, 1, 21, 11, None) == 2
+    # unknown operator
+    assert _capi.lib.sbp_interpolate(7, 1, _capi.F64, p, p, 41, 21, 1, 41, 21, None) == 1

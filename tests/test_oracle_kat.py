@@ -194,3 +194,45 @@ def test_convergence(orc, op_name, expected_q):
             q_last = q
         prev = (size, e)
     assert q_last < expected_q, q_last
+
+
+# ---- interpolation operators (sbp/src/operators/interpolation*.rs) -------------------------
+def _ndarray_linspace(a, b, n):
+    step = (b - a) / (n - 1)
+    return a + step * np.arange(n)
+
+
+@pytest.mark.parametrize("op,h2", [(0, False), (1, False), (2, False), (3, True)])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-11), (np.float32, 1e-4)])
+def test_interpolation_exact_on_linear(orc, op, h2, dtype, tol):
+    """test_interpolation_operator (interpolation.rs:52-74): coarse2fine and fine2coarse of a
+    linear function (the grid itself) are exact to 1e-11 (f64; the f32 build to its precision:
+    the values are about 50, so 1e-4 relative covers a few f32 ulps)."""
+    nc = 101
+    if h2:
+        xc, xf = h2linspace(20.0, 50.0, nc), h2linspace(20.0, 50.0, 2 * (nc - 1))
+    else:
+        xc, xf = _ndarray_linspace(20.0, 50.0, 101), _ndarray_linspace(20.0, 50.0, 2 * nc - 1)
+    xc, xf = xc.astype(dtype), xf.astype(dtype)
+    f = orc.interpolate(op, False, xc, dtype)
+    c = orc.interpolate(op, True, xf, dtype)
+    scale = 1.0 if dtype == np.float64 else 50.0
+    assert np.max(np.abs(f - xf)) <= tol * scale
+    assert np.max(np.abs(c - xc)) <= tol * scale
+
+
+def test_interpolation_tables_identical():
+    """The library's and the oracle's interpolation tables (two headers written by
+    oracle/gen_interp_coefficients.py) hold the same numbers."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    a = open(os.path.join(root, "summationbyparts_b200", "csrc", "interp_coefficients.h")).read()
+    b = open(os.path.join(root, "oracle", "oracle_interp_coefficients.h")).read()
+    da = dict(re.findall(r"#define SBPI_(\w+) ([^\n]*)", a))
+    db = dict(re.findall(r"#define ORCI_(\w+) ([^\n]*)", b))
+    assert da.keys() == db.keys() and len(da) == 4 * (2 * 10 + 1)
+    for k in da:
+        va = [float(v.strip().rstrip("f")) for v in da[k].split("//")[0].split(",")]
+        vb = [float(v.strip().rstrip("f")) for v in db[k].split("//")[0].split(",")]
+        assert va == vb, k
