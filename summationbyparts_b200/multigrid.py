@@ -5,11 +5,12 @@ Mirrors the reference's multigrid driver (multigrid/src/system.rs:368-636):
     dt = sys.max_dt(); sys.set_dt(dt)
     sys.advance(nsteps)
     err = sys.error()                       # sum over blocks of h2_err vs the vortex
-Boundary characteristics per side are BoundaryCharacteristic values: THIS (own opposite
-edge), ("grid", g) (block g's opposite edge) or VORTEX (exact vortex data at stage time),
-euler/src/lib.rs:737-745, 869-930.  Grids with fine = 2*coarse-1 interpolation or
-multi-neighbour edges are not supported (the single-threaded driver also rejects nothing
-here: the library returns SBP_ERR_SHAPE for unequal interface lengths).
+Boundary characteristics per side are BoundaryCharacteristic values (euler/src/lib.rs:737-745,
+804-930): THIS (own opposite edge), ("grid", g) (block g's opposite edge), VORTEX (exact vortex
+data at stage time), ("interpolate", g, op) (block g's opposite edge through a 2:1
+interpolation operator, op 0..3 = Interpolation4, 8, 9, 9h2) and ("multi", [(g, start, end),
+...]) (segments of several blocks' opposite edges).  The library returns SBP_ERR_SHAPE for
+interfaces whose lengths do not fit.
 """
 from __future__ import annotations
 
@@ -17,7 +18,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._capi import BC_GRID, BC_THIS, BC_VORTEX
+from ._capi import BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX
 from .system import BlockSpec, BlockSystem, VortexParameters
 
 THIS = "this"
@@ -26,6 +27,14 @@ VORTEX = "vortex"
 
 def grid_bc(g: int):
     return ("grid", g)
+
+
+def interpolate_bc(g: int, op: int):
+    return ("interpolate", g, op)
+
+
+def multi_bc(segments):
+    return ("multi", [tuple(int(v) for v in sgm) for sgm in segments])
 
 
 @dataclass
@@ -47,18 +56,28 @@ def _bc(v):
         return (BC_VORTEX, 0)
     if isinstance(v, tuple) and v[0] == "grid":
         return (BC_GRID, int(v[1]))
+    if isinstance(v, tuple) and v[0] == "interpolate":
+        return (BC_INTERPOLATE, int(v[1]), int(v[2]))
+    if isinstance(v, tuple) and v[0] == "multi":
+        return (BC_MULTIGRID, list(v[1]))
     raise ValueError(f"unsupported boundary characteristic {v!r}")
 
 
 class System:
     def __init__(self, grids: list[Grid], vortex: VortexParameters, gamma: float = 1.4, precision: str = "f64",
-                 device: int = 0, time: float = 0.0):
+                 device: int = 0, time: float = 0.0, boundary_vortex: VortexParameters | None = None):
+        """vortex: the initial conditions (and the exact solution of error()); boundary_vortex:
+        the vortex of VORTEX sides when it differs from the initial one."""
         specs = [BlockSpec(g.x, g.y, g.op, [_bc(g.north), _bc(g.south), _bc(g.east), _bc(g.west)], 0) for g in grids]
         self.grids = grids
+        self.vortex = vortex
+        self.boundary_vortex = boundary_vortex or vortex
         self._sys = BlockSystem(specs, 1, precision, gamma, device)
         self._sys.set_vortex(vortex)
         self._sys.init_vortex(time)
         self._sys.set_time(time)
+        if self.boundary_vortex is not vortex:
+            self._sys.set_vortex(self.boundary_vortex)
 
     def max_dt(self) -> float:
         return self._sys.max_dt(0)
@@ -70,6 +89,13 @@ class System:
         self._sys.advance(nsteps)
 
     def error(self) -> float:
+        """Sum over blocks of h2_err against the initial-condition vortex at the current time
+        (multigrid/src/system.rs:618-635)."""
+        if self.boundary_vortex is not self.vortex:
+            self._sys.set_vortex(self.vortex)
+            e = float(self._sys.errors()[0])
+            self._sys.set_vortex(self.boundary_vortex)
+            return e
         return float(self._sys.errors()[0])
 
     @property
