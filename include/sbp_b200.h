@@ -233,6 +233,30 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads);
 sbp_status sbp_system_set_stream(sbp_system* sys, void* stream);
 /* Device pointer to one block's current state plane set (f64 or f32 hi), for zero-copy use. */
 sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q);
+/* Explicit Runge-Kutta tableaus of utils/integrate/src/lib.rs:30-152. */
+typedef enum sbp_tableau {
+    SBP_RK4 = 0,
+    SBP_RK4_38 = 1,
+    SBP_EULER_METHOD = 2,
+    SBP_MIDPOINT_METHOD = 3,
+    SBP_RK6 = 4,
+    SBP_FEHLBERG = 5,
+    SBP_BOGACKI_SHAMPINE = 6
+} sbp_tableau;
+/* nsteps steps of integrate::<tableau> (utils/integrate/src/lib.rs:176-222) with each instance's
+ * dt: k_i = RHS(prev + sum_j (a_ij dt) k_j) for every stage (the stage and edge kernels in a
+ * k-only mode, SATs at time + dt c_i), then prev + sum_j (b_j dt) k_j, all in the reference's
+ * order of operations; time += dt.  f64 systems only (SBP_ERR_UNSUPPORTED otherwise); every
+ * instance takes part.  sbp_system_advance remains the fused RK4 path. */
+sbp_status sbp_system_advance_tableau(sbp_system* sys, int tableau, int64_t nsteps);
+/* euler::System::advance_adaptive (euler/src/lib.rs:149-186) for a single-block f64 system
+ * whose four sides are SBP_BC_THIS: embedded Bogacki-Shampine steps of *guess_dt until the
+ * local time reaches dt; a step is kept when h2_err(prev, low-order result) < maxerr, and
+ * *guess_dt grows by 1.05 after a kept step and shrinks by 0.8 after a rejected one (the time
+ * bookkeeping and the compared states are the reference's, as written).  The instance time is
+ * not advanced (the reference's euler::System has none). */
+sbp_status sbp_system_advance_adaptive(sbp_system* sys, double dt, double* guess_dt, double maxerr);
+
 /* Kernel launches per RK4 step: per operator pair and stage a stage kernel and an edge (SAT)
  * kernel, plus the time update. */
 int sbp_system_launches_per_step(const sbp_system* sys);

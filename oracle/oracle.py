@@ -90,6 +90,10 @@ def lib(fast: bool = False) -> ctypes.CDLL:
     L.orc_system_get_state.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
     L.orc_system_get_metrics.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
     L.orc_system_advance.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int]
+    L.orc_system_advance_tableau.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double,
+                                             ctypes.c_int]
+    L.orc_system_advance_adaptive.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.c_double]
     L.orc_system_time.argtypes = [ctypes.c_void_p]
     L.orc_system_time.restype = ctypes.c_double
     L.orc_system_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double]
@@ -291,6 +295,20 @@ class System:
     @time.setter
     def time(self, t):
         self._L.orc_system_set_time(self.h, t)
+
+    def advance_tableau(self, tableau: int, nsteps: int, dt: float, force_trad: bool = False):
+        """integrate::<tableau> steps: 0 Rk4, 1 Rk4_38, 2 EulerMethod, 3 MidpointMethod, 4 Rk6,
+        5 Fehlberg, 6 BogackiShampine."""
+        rc = self._L.orc_system_advance_tableau(self.h, tableau, nsteps, dt, int(force_trad))
+        if rc:
+            raise RuntimeError(f"orc_system_advance_tableau: {rc}")
+
+    def advance_adaptive(self, dt: float, guess_dt: float, maxerr: float) -> float:
+        g = ctypes.c_double(guess_dt)
+        rc = self._L.orc_system_advance_adaptive(self.h, dt, ctypes.byref(g), maxerr)
+        if rc:
+            raise RuntimeError(f"orc_system_advance_adaptive: {rc}")
+        return g.value
 
     def max_dt(self) -> float:
         return self._L.orc_system_max_dt(self.h)

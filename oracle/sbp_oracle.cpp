@@ -594,7 +594,7 @@ struct orc_system {
     std::vector<Metrics> metrics;
     std::vector<BlockCtx> ctx;
     std::vector<std::vector<double>> now, fut;
-    std::vector<std::vector<double>> k[4];
+    std::vector<std::vector<double>> k[8];
     std::vector<Work> work;
     std::vector<std::vector<double>> ebuf[4];
     orc_vortex_params vp{};
@@ -812,6 +812,138 @@ static int advance_step(orc_system* s, double dt, bool force_trad) {
     return bad ? -4 : 0;
 }
 
+/* The Butcher tableaus of utils/integrate/src/lib.rs:30-152 (A by rows of stages 2..S). */
+struct OrcTableau {
+    int s;
+    double a[8][8];
+    double b[8], c[8], bstar[8];
+};
+static std::vector<OrcTableau> orc_tableaus() {
+    const double R5 = 2.236067977499789696409173668731276235440618359611525724270897245410520925637804899414414408378782275;
+    std::vector<OrcTableau> t(7);
+    for (auto& x : t) std::memset(&x, 0, sizeof x);
+    // 0 Rk4
+    t[0].s = 4;
+    t[0].a[0][0] = 0.5;
+    t[0].a[1][1] = 0.5;
+    t[0].a[2][2] = 1.0;
+    t[0].b[0] = 1.0 / 6.0; t[0].b[1] = 1.0 / 3.0; t[0].b[2] = 1.0 / 3.0; t[0].b[3] = 1.0 / 6.0;
+    t[0].c[0] = 0.5; t[0].c[1] = 0.5; t[0].c[2] = 1.0;
+    // 1 Rk4_38
+    t[1].s = 4;
+    t[1].a[0][0] = 1.0 / 3.0;
+    t[1].a[1][0] = -1.0 / 3.0; t[1].a[1][1] = 1.0;
+    t[1].a[2][0] = 1.0; t[1].a[2][1] = -1.0; t[1].a[2][2] = 1.0;
+    t[1].b[0] = 1.0 / 8.0; t[1].b[1] = 3.0 / 8.0; t[1].b[2] = 3.0 / 8.0; t[1].b[3] = 1.0 / 8.0;
+    t[1].c[0] = 1.0 / 3.0; t[1].c[1] = 2.0 / 3.0; t[1].c[2] = 1.0;
+    // 2 EulerMethod
+    t[2].s = 1;
+    t[2].b[0] = 1.0;
+    // 3 MidpointMethod
+    t[3].s = 2;
+    t[3].a[0][0] = 0.5;
+    t[3].b[1] = 1.0;
+    t[3].c[0] = 1.0 / 2.0;
+    // 4 Rk6
+    t[4].s = 7;
+    t[4].a[0][0] = 4.0 / 7.0;
+    t[4].a[1][0] = 115.0 / 112.0; t[4].a[1][1] = -5.0 / 16.0;
+    t[4].a[2][0] = 589.0 / 630.0; t[4].a[2][1] = 5.0 / 18.0; t[4].a[2][2] = -16.0 / 45.0;
+    t[4].a[3][0] = 229.0 / 1200.0 - 29.0 / 6000.0 * R5;
+    t[4].a[3][1] = 119.0 / 240.0 - 187.0 / 1200.0 * R5;
+    t[4].a[3][2] = -14.0 / 75.0 + 34.0 / 375.0 * R5;
+    t[4].a[3][3] = -3.0 / 100.0 * R5;
+    t[4].a[4][0] = 71.0 / 2400.0 - 587.0 / 12000.0 * R5;
+    t[4].a[4][1] = 187.0 / 480.0 - 391.0 / 2400.0 * R5;
+    t[4].a[4][2] = -38.0 / 75.0 + 26.0 / 375.0 * R5;
+    t[4].a[4][3] = 27.0 / 80.0 - 3.0 / 400.0 * R5;
+    t[4].a[4][4] = (1.0 + R5) / 4.0;
+    t[4].a[5][0] = -49.0 / 480.0 + 43.0 / 160.0 * R5;
+    t[4].a[5][1] = -425.0 / 96.0 + 51.0 / 32.0 * R5;
+    t[4].a[5][2] = 52.0 / 15.0 - 4.0 / 5.0 * R5;
+    t[4].a[5][3] = -27.0 / 16.0 + 3.0 / 16.0 * R5;
+    t[4].a[5][4] = 5.0 / 4.0 - 3.0 / 4.0 * R5;
+    t[4].a[5][5] = 5.0 / 2.0 - 1.0 / 2.0 * R5;
+    t[4].b[0] = 1.0 / 12.0; t[4].b[4] = 5.0 / 12.0; t[4].b[5] = 5.0 / 12.0; t[4].b[6] = 1.0 / 12.0;
+    t[4].c[0] = 4.0 / 7.0; t[4].c[1] = 5.0 / 7.0; t[4].c[2] = 6.0 / 7.0;
+    t[4].c[3] = (5.0 - R5) / 10.0; t[4].c[4] = (5.0 + R5) / 10.0; t[4].c[5] = 1.0;
+    // 5 Fehlberg
+    t[5].s = 6;
+    t[5].a[0][0] = 1.0 / 4.0;
+    t[5].a[1][0] = 3.0 / 32.0; t[5].a[1][1] = 9.0 / 32.0;
+    t[5].a[2][0] = 1932.0 / 2197.0; t[5].a[2][1] = -7200.0 / 2197.0; t[5].a[2][2] = 7296.0 / 2197.0;
+    t[5].a[3][0] = 439.0 / 216.0; t[5].a[3][1] = -8.0; t[5].a[3][2] = 3680.0 / 513.0; t[5].a[3][3] = -845.0 / 4104.0;
+    t[5].a[4][0] = -8.0 / 27.0; t[5].a[4][1] = 2.0; t[5].a[4][2] = -3544.0 / 2565.0; t[5].a[4][3] = 1859.0 / 4104.0;
+    t[5].a[4][4] = -11.0 / 40.0;
+    t[5].b[0] = 16.0 / 135.0; t[5].b[2] = 6656.0 / 12825.0; t[5].b[3] = 28561.0 / 56430.0; t[5].b[4] = -9.0 / 50.0;
+    t[5].b[5] = 2.0 / 55.0;
+    t[5].c[1] = 1.0 / 4.0; t[5].c[2] = 3.0 / 8.0; t[5].c[3] = 12.0 / 13.0; t[5].c[4] = 1.0; t[5].c[5] = 1.0 / 2.0;
+    t[5].bstar[0] = 25.0 / 216.0; t[5].bstar[2] = 1408.0 / 2565.0; t[5].bstar[3] = 2197.0 / 4104.0;
+    t[5].bstar[4] = -1.0 / 5.0;
+    // 6 BogackiShampine
+    t[6].s = 4;
+    t[6].a[0][0] = 1.0 / 2.0;
+    t[6].a[1][1] = 3.0 / 4.0;
+    t[6].a[2][0] = 2.0 / 9.0; t[6].a[2][1] = 1.0 / 3.0; t[6].a[2][2] = 4.0 / 9.0;
+    t[6].b[0] = 2.0 / 9.0; t[6].b[1] = 1.0 / 3.0; t[6].b[2] = 4.0 / 9.0;
+    t[6].c[1] = 1.0 / 2.0; t[6].c[2] = 3.0 / 4.0; t[6].c[3] = 1.0;
+    t[6].bstar[0] = 7.0 / 24.0; t[6].bstar[1] = 1.0 / 4.0; t[6].bstar[2] = 1.0 / 3.0; t[6].bstar[3] = 1.0 / 8.0;
+    return t;
+}
+
+/* integrate (utils/integrate/src/lib.rs:176-222) and, when fut2 is given,
+ * integrate_embedded_rk's second combination (:237-251); the result goes to s->fut. */
+static int integrate_general(orc_system* s, const OrcTableau& T, double dt, bool force_trad, double& time,
+                             std::vector<std::vector<double>>* fut2) {
+    const size_t nb = s->desc.size();
+    int bad = 0;
+    for (int i = 0; i < T.s; ++i) {
+        for (size_t b = 0; b < nb; ++b) {
+            s->fut[b] = s->now[b];
+            for (int j = 0; j < i; ++j) {
+                const double a = T.a[i - 1][j];
+                if (a == 0.0) continue;
+                const double sc = a * dt;
+                std::vector<double>& f = s->fut[b];
+                const std::vector<double>& kk = s->k[j][b];
+                for (size_t q = 0; q < f.size(); ++q) f[q] = f[q] + sc * kk[q];
+            }
+        }
+        const double simtime = i == 0 ? time : time + dt * T.c[i - 1];
+        for (size_t b = 0; b < nb; ++b) {
+            const double* z[4];
+            int rc = extract(s, s->fut, (int)b, simtime, z);
+            if (rc) return rc;
+            bad |= rhs(s->ctx[b], s->gamma, s->fut[b].data(), z, force_trad, s->k[i][b].data(), s->work[b]);
+        }
+    }
+    for (size_t b = 0; b < nb; ++b) {
+        std::vector<double>& f = s->fut[b];
+        f = s->now[b];
+        for (int j = 0; j < T.s; ++j) {
+            if (T.b[j] == 0.0) continue;
+            const double sc = T.b[j] * dt;
+            const std::vector<double>& kk = s->k[j][b];
+            for (size_t q = 0; q < f.size(); ++q) f[q] = f[q] + sc * kk[q];
+        }
+    }
+    time += dt;
+    if (fut2) {
+        fut2->resize(nb);
+        for (size_t b = 0; b < nb; ++b) {
+            std::vector<double>& f = (*fut2)[b];
+            f = s->now[b];
+            for (int j = 0; j < T.s; ++j) {
+                if (T.bstar[j] == 0.0) continue;
+                const double sc = T.bstar[j] * dt;
+                const std::vector<double>& kk = s->k[j][b];
+                for (size_t q = 0; q < f.size(); ++q) f[q] = f[q] + sc * kk[q];
+            }
+        }
+    }
+    return bad ? -4 : 0;
+}
+
 }  // namespace
 
 /* ------------------------------------------------------------------------- */
@@ -994,6 +1126,41 @@ int orc_system_advance(orc_system* s, int64_t nsteps, double dt, int force_trad)
     for (int64_t i = 0; i < nsteps; ++i) {
         int rc = advance_step(s, dt, force_trad != 0);
         if (rc) return rc;
+    }
+    return 0;
+}
+
+int orc_system_advance_tableau(orc_system* s, int tableau, int64_t nsteps, double dt, int force_trad) {
+    static const std::vector<OrcTableau> tabs = orc_tableaus();
+    if (tableau < 0 || tableau >= (int)tabs.size()) return -1;
+    for (int64_t i = 0; i < nsteps; ++i) {
+        int rc = integrate_general(s, tabs[tableau], dt, force_trad != 0, s->time, nullptr);
+        if (rc) return rc;
+        std::swap(s->now, s->fut);
+    }
+    return 0;
+}
+
+/* euler::System::advance_adaptive (euler/src/lib.rs:149-186), as written: a local time starting
+ * at 0 that integrate advances by the step and an accepted step advances once more; the error
+ * is h2_err of the previous state against the low-order result.  Single block. */
+int orc_system_advance_adaptive(orc_system* s, double dt, double* guess_dt, double maxerr) {
+    static const std::vector<OrcTableau> tabs = orc_tableaus();
+    if (s->desc.size() != 1) return -1;
+    const orc_block_desc& D = s->desc[0];
+    std::vector<std::vector<double>> sys2;
+    double time = 0.0;
+    while (time < dt) {
+        int rc = integrate_general(s, tabs[6], *guess_dt, false, time, &sys2);
+        if (rc) return rc;
+        const double err = orc_h2_err(D.op_xi, D.op_eta, s->now[0].data(), sys2[0].data(), D.ny, D.nx);
+        if (err < maxerr) {
+            time += *guess_dt;
+            std::swap(s->now, s->fut);
+            *guess_dt *= 1.05;
+        } else {
+            *guess_dt *= 0.8;
+        }
     }
     return 0;
 }

@@ -85,6 +85,12 @@ int orc_rhs(int op_xi, int op_eta, double gamma, const double* q, const double* 
  * break the operator's assert (fine = 2 coarse - 1, or 2 (coarse - 1) for 9h2). */
 int orc_interpolate(int op, int fine2coarse, int dtype, const void* in, int64_t n_in, void* out, int64_t n_out);
 
+/* integrate::<tableau> steps (0 Rk4, 1 Rk4_38, 2 EulerMethod, 3 MidpointMethod, 4 Rk6,
+ * 5 Fehlberg, 6 BogackiShampine; utils/integrate/src/lib.rs:30-222) and
+ * euler::System::advance_adaptive (euler/src/lib.rs:149-186) on a system. */
+int orc_system_advance_tableau(orc_system* s, int tableau, int64_t nsteps, double dt, int force_trad);
+int orc_system_advance_adaptive(orc_system* s, double dt, double* guess_dt, double maxerr);
+
 /* Field::h2_err (euler/src/lib.rs:377-431) */
 double orc_h2_err(int op_xi, int op_eta, const double* a, const double* b, int64_t ny, int64_t nx);
 

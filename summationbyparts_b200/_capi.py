@@ -20,6 +20,7 @@ F64, F32 = 0, 1
 PRECISION_F64, PRECISION_F32_COMPENSATED = 0, 1
 BC_THIS, BC_GRID, BC_VORTEX, BC_INTERPOLATE, BC_MULTIGRID = 0, 1, 2, 3, 4
 INTERP4, INTERP8, INTERP9, INTERP9H2 = 0, 1, 2, 3
+TABLEAUS = {"rk4": 0, "rk4_38": 1, "euler": 2, "midpoint": 3, "rk6": 4, "fehlberg": 5, "bogacki_shampine": 6}
 NORTH, SOUTH, EAST, WEST = 0, 1, 2, 3
 
 
@@ -86,6 +87,8 @@ SIGNATURES = {
     "sbp_system_set_stream": (_i, [_vp, _vp]),
     "sbp_system_device_state": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
     "sbp_system_launches_per_step": (_i, [_vp]),
+    "sbp_system_advance_tableau": (_i, [_vp, _i, _i64]),
+    "sbp_system_advance_adaptive": (_i, [_vp, _d, _dp, _d]),
     "sbp_system_group_count": (_i, [_vp]),
     "sbp_system_group_info": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i64)]),
     "sbp_system_launch_stage": (_i, [_vp, _i, _i, _i]),

@@ -52,7 +52,8 @@ struct StageArgs {
     const InstanceDev* __restrict__ inst;
     const int4* __restrict__ tiles;
     int ntiles;
-    int stage;               // 0..3
+    int stage;               // 0..3 (RK4), or kStageK: write k to u_out (other tableaus)
+    double ctime;            // kStageK: the stage's C coefficient (SAT data at time + dt * ctime)
     const T* u_in;           // stage input state, all blocks
     const T* prev_hi;        // state at the start of the step
     const T* prev_lo;        // low part of the state (compensated precision only)
@@ -70,6 +71,10 @@ struct StageArgs {
     double gamma;
     unsigned* status;
 };
+
+// Stage index of the k-only mode: the launch computes k = RHS(u_in) (SATs included) into u_out
+// and updates nothing else; explicit tableaus other than RK4 combine the k on the host side.
+constexpr int kStageK = 4;
 
 // Device coefficient table (one per precision): for operator o and kind k the rows
 // [start block M rows][end block M rows][interior diagonal], each row padded to kCoefRow
@@ -415,6 +420,10 @@ __device__ __forceinline__ int stage_operands(const StageArgs<T>& A, const T* sr
 // as rk_update.  cb, ca: this stage's B and A tableau entries times dt, already in f32.
 template <class T, class SOP>
 __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, int64_t e, float cb, float ca, T kc, SOP sop) {
+    if (A.stage == kStageK) {
+        A.u_out[e] = kc;
+        return;
+    }
     const float kf = float(kc);
     if (A.stage == 0) {
         float hi = float(sop(1));
@@ -445,6 +454,10 @@ __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, int64_t 
 // stage 0); cb, ca: this stage's B and A tableau entries times dt (ca unused in stage 3).
 template <class T, bool COMP>
 __device__ __forceinline__ void rk_update(const StageArgs<T>& A, int64_t e, T qv, T kc, double cb, double ca) {
+    if (A.stage == kStageK) {
+        A.u_out[e] = kc;
+        return;
+    }
     if constexpr (!COMP) {
         const T cbt = T(cb);
         if (A.stage == 0) {
@@ -503,8 +516,8 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
     const int64_t np = B.npad;
     const bool on[4] = {row == ny - 1, row == 0, col == nx - 1, col == 0};
     const double* m64 = A.met64 + B.m_off;
-    const double cst = A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5);
-    const double stime = A.stage == 0 ? I.time : I.time + I.dt * cst;
+    const double cst = A.stage == kStageK ? A.ctime : (A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5));
+    const double stime = cst == 0.0 ? I.time : I.time + I.dt * cst;
     for (int d = 0; d < 4; ++d) {
         if (!on[d]) continue;
         double zv[4];
@@ -606,7 +619,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         const T* q = A.u_in + qoff;
         const T* mt = A.met + B.m_off;
         const InstanceDev& I = A.inst[B.instance];
-        const double cb = I.cb[A.stage];
+        const double cb = A.stage < 4 ? I.cb[A.stage] : 0.0;
         const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
 
         // ---------------- phase 1: pointwise quantities ----------------
@@ -768,7 +781,7 @@ __global__ void __launch_bounds__(kSatThreads) sat_kernel(const StageArgs<T> A, 
     const int nx = B.nx, ny = B.ny;
     const int64_t np = B.npad, qoff = B.q_off;
     const int64_t slot = 4 * (B.e_off + edge_index(row, col, nx, ny));
-    const double cb = I.cb[A.stage];
+    const double cb = A.stage < 4 ? I.cb[A.stage] : 0.0;
     const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
     const int pt = row * nx + col;
     const T* q = A.u_in + qoff;

@@ -119,6 +119,8 @@ struct sbp_system {
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
+    double* kbuf = nullptr;  // k of the stages of a general tableau (kMaxStages x nq, f64), on demand
+    int kbuf_stages = 0;
     // schedule
     int TY = 16, TX = kTileX, threads = kStageThreads;
     std::vector<int> active;
@@ -159,7 +161,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -251,6 +253,101 @@ sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t s
         if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     }
     return cuda_status(e, "stage kernel launch");
+}
+
+// Butcher tableaus of utils/integrate/src/lib.rs:30-152 (explicit; A lower triangle by rows of
+// stages 2..S, then B, C and, for the embedded ones, BSTAR).  The values are the reference's
+// constant expressions, evaluated in f64 as its compiler does (one rounding per operation).
+struct Tableau {
+    int s;
+    double a[kMaxStages][kMaxStages];  // a[i][j]: stage i+1 (1-based 2..S), j < i+1
+    double b[kMaxStages];
+    double c[kMaxStages];
+    double bstar[kMaxStages];
+    bool embedded;
+};
+
+std::vector<Tableau> make_tableaus() {
+    std::vector<Tableau> t(7);
+    {
+        const double SQRT_5 = 2.236067977499789696409173668731276235440618359611525724270897245410520925637804899414414408378782275;
+        for (auto& x : t) std::memset(&x, 0, sizeof x);
+        // Rk4
+        t[0].s = 4;
+        t[0].a[0][0] = 0.5;
+        t[0].a[1][0] = 0.0, t[0].a[1][1] = 0.5;
+        t[0].a[2][0] = 0.0, t[0].a[2][1] = 0.0, t[0].a[2][2] = 1.0;
+        t[0].b[0] = 1.0 / 6.0, t[0].b[1] = 1.0 / 3.0, t[0].b[2] = 1.0 / 3.0, t[0].b[3] = 1.0 / 6.0;
+        t[0].c[0] = 0.5, t[0].c[1] = 0.5, t[0].c[2] = 1.0;
+        // Rk4_38
+        t[1].s = 4;
+        t[1].a[0][0] = 1.0 / 3.0;
+        t[1].a[1][0] = -1.0 / 3.0, t[1].a[1][1] = 1.0;
+        t[1].a[2][0] = 1.0, t[1].a[2][1] = -1.0, t[1].a[2][2] = 1.0;
+        t[1].b[0] = 1.0 / 8.0, t[1].b[1] = 3.0 / 8.0, t[1].b[2] = 3.0 / 8.0, t[1].b[3] = 1.0 / 8.0;
+        t[1].c[0] = 1.0 / 3.0, t[1].c[1] = 2.0 / 3.0, t[1].c[2] = 1.0;
+        // EulerMethod
+        t[2].s = 1;
+        t[2].b[0] = 1.0;
+        // MidpointMethod
+        t[3].s = 2;
+        t[3].a[0][0] = 0.5;
+        t[3].b[0] = 0.0, t[3].b[1] = 1.0;
+        t[3].c[0] = 1.0 / 2.0;
+        // Rk6
+        t[4].s = 7;
+        t[4].a[0][0] = 4.0 / 7.0;
+        t[4].a[1][0] = 115.0 / 112.0, t[4].a[1][1] = -5.0 / 16.0;
+        t[4].a[2][0] = 589.0 / 630.0, t[4].a[2][1] = 5.0 / 18.0, t[4].a[2][2] = -16.0 / 45.0;
+        t[4].a[3][0] = 229.0 / 1200.0 - 29.0 / 6000.0 * SQRT_5;
+        t[4].a[3][1] = 119.0 / 240.0 - 187.0 / 1200.0 * SQRT_5;
+        t[4].a[3][2] = -14.0 / 75.0 + 34.0 / 375.0 * SQRT_5;
+        t[4].a[3][3] = -3.0 / 100.0 * SQRT_5;
+        t[4].a[4][0] = 71.0 / 2400.0 - 587.0 / 12000.0 * SQRT_5;
+        t[4].a[4][1] = 187.0 / 480.0 - 391.0 / 2400.0 * SQRT_5;
+        t[4].a[4][2] = -38.0 / 75.0 + 26.0 / 375.0 * SQRT_5;
+        t[4].a[4][3] = 27.0 / 80.0 - 3.0 / 400.0 * SQRT_5;
+        t[4].a[4][4] = (1.0 + SQRT_5) / 4.0;
+        t[4].a[5][0] = -49.0 / 480.0 + 43.0 / 160.0 * SQRT_5;
+        t[4].a[5][1] = -425.0 / 96.0 + 51.0 / 32.0 * SQRT_5;
+        t[4].a[5][2] = 52.0 / 15.0 - 4.0 / 5.0 * SQRT_5;
+        t[4].a[5][3] = -27.0 / 16.0 + 3.0 / 16.0 * SQRT_5;
+        t[4].a[5][4] = 5.0 / 4.0 - 3.0 / 4.0 * SQRT_5;
+        t[4].a[5][5] = 5.0 / 2.0 - 1.0 / 2.0 * SQRT_5;
+        t[4].b[0] = 1.0 / 12.0, t[4].b[4] = 5.0 / 12.0, t[4].b[5] = 5.0 / 12.0, t[4].b[6] = 1.0 / 12.0;
+        t[4].c[0] = 4.0 / 7.0, t[4].c[1] = 5.0 / 7.0, t[4].c[2] = 6.0 / 7.0;
+        t[4].c[3] = (5.0 - SQRT_5) / 10.0, t[4].c[4] = (5.0 + SQRT_5) / 10.0, t[4].c[5] = 1.0;
+        // Fehlberg (C has S entries: C[i - 1] is used for stage i as in the other tableaus)
+        t[5].s = 6;
+        t[5].a[0][0] = 1.0 / 4.0;
+        t[5].a[1][0] = 3.0 / 32.0, t[5].a[1][1] = 9.0 / 32.0;
+        t[5].a[2][0] = 1932.0 / 2197.0, t[5].a[2][1] = -7200.0 / 2197.0, t[5].a[2][2] = 7296.0 / 2197.0;
+        t[5].a[3][0] = 439.0 / 216.0, t[5].a[3][1] = -8.0, t[5].a[3][2] = 3680.0 / 513.0, t[5].a[3][3] = -845.0 / 4104.0;
+        t[5].a[4][0] = -8.0 / 27.0, t[5].a[4][1] = 2.0, t[5].a[4][2] = -3544.0 / 2565.0, t[5].a[4][3] = 1859.0 / 4104.0;
+        t[5].a[4][4] = -11.0 / 40.0;
+        t[5].b[0] = 16.0 / 135.0, t[5].b[2] = 6656.0 / 12825.0, t[5].b[3] = 28561.0 / 56430.0, t[5].b[4] = -9.0 / 50.0;
+        t[5].b[5] = 2.0 / 55.0;
+        t[5].c[0] = 0.0, t[5].c[1] = 1.0 / 4.0, t[5].c[2] = 3.0 / 8.0, t[5].c[3] = 12.0 / 13.0, t[5].c[4] = 1.0;
+        t[5].c[5] = 1.0 / 2.0;
+        t[5].bstar[0] = 25.0 / 216.0, t[5].bstar[2] = 1408.0 / 2565.0, t[5].bstar[3] = 2197.0 / 4104.0;
+        t[5].bstar[4] = -1.0 / 5.0;
+        t[5].embedded = true;
+        // BogackiShampine
+        t[6].s = 4;
+        t[6].a[0][0] = 1.0 / 2.0;
+        t[6].a[1][0] = 0.0, t[6].a[1][1] = 3.0 / 4.0;
+        t[6].a[2][0] = 2.0 / 9.0, t[6].a[2][1] = 1.0 / 3.0, t[6].a[2][2] = 4.0 / 9.0;
+        t[6].b[0] = 2.0 / 9.0, t[6].b[1] = 1.0 / 3.0, t[6].b[2] = 4.0 / 9.0, t[6].b[3] = 0.0;
+        t[6].c[0] = 0.0, t[6].c[1] = 1.0 / 2.0, t[6].c[2] = 3.0 / 4.0, t[6].c[3] = 1.0;
+        t[6].bstar[0] = 7.0 / 24.0, t[6].bstar[1] = 1.0 / 4.0, t[6].bstar[2] = 1.0 / 3.0, t[6].bstar[3] = 1.0 / 8.0;
+        t[6].embedded = true;
+    }
+    return t;
+}
+
+const Tableau* tableau_of(int id) {
+    static const std::vector<Tableau> t = make_tableaus();  // thread-safe initialisation
+    return id >= 0 && id < 7 ? &t[id] : nullptr;
 }
 
 // Build per-operator-pair tile lists for the active blocks, size shared memory and grids.
@@ -406,6 +503,80 @@ sbp_status run_steps(sbp_system* s, int64_t n) {
 }
 
 bool valid_block(const sbp_system* s, int b) { return b >= 0 && b < s->nblocks; }
+
+// k = RHS(u_in) (SATs included) into k_out for every group: the stage and edge kernels in their
+// k-only mode, SAT data at time + dt * ctime.
+sbp_status launch_rhs(sbp_system* s, const double* u_in, double* k_out, double ctime) {
+    cudaStream_t st = s->st();
+    for (const Group& g : s->groups) {
+        if (g.ntiles == 0) continue;
+        StageArgs<double> a = stage_args<double>(s, 0, g);
+        a.stage = kStageK;
+        a.ctime = ctime;
+        a.u_in = u_in;
+        a.u_out = k_out;
+        void* args[] = {&a};
+        SBP_TRY_CUDA(cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st));
+        int4* edges = g.d_edges;
+        int nedges = g.nedges;
+        void* sargs[] = {&a, &edges, &nedges};
+        SBP_TRY_CUDA(cudaLaunchKernel(sat_ptr_f64(), dim3((g.nedges + kSatThreads - 1) / kSatThreads),
+                                      dim3(kSatThreads), sargs, 0, st));
+    }
+    return SBP_OK;
+}
+
+sbp_status ensure_kbuf(sbp_system* s, int stages) {
+    if (s->kbuf_stages >= stages) return SBP_OK;
+    if (s->kbuf) cudaFree(s->kbuf);
+    s->kbuf = nullptr;
+    s->kbuf_stages = 0;
+    SBP_TRY_CUDA(cudaMalloc((void**)&s->kbuf, (size_t)kMaxStages * s->nq * sizeof(double)));
+    s->kbuf_stages = kMaxStages;
+    return SBP_OK;
+}
+
+// integrate::<Tableau> (utils/integrate/src/lib.rs:176-222) for every block: the stage inputs
+// fut = prev; fut += (a dt) k_j in order, the RHS of each stage into its k, and at the end
+// prev = prev + (b dt) k_j in order (in place).  dt_fixed < 0: each instance's own dt.
+// Embedded tableaus also form fut2 = prev + (bstar dt) k_j into `fut2` when it is given and
+// leave prev untouched, writing the B combination to `fut` instead.
+sbp_status integrate_tableau(sbp_system* s, const Tableau& T, double dt_fixed, double* fut, double* fut2) {
+    cudaStream_t st = s->st();
+    double* prev = static_cast<double*>(s->prev_hi);
+    double* stage_in = static_cast<double*>(s->uA);
+    auto kk = [&](int j) { return s->kbuf + (size_t)j * s->nq; };
+    for (int i = 0; i < T.s; ++i) {
+        const double* in = prev;
+        double ctime = 0.0;
+        if (i > 0) {
+            StageCombination cm{};
+            for (int j = 0; j < i; ++j) {
+                cm.coef[j] = T.a[i - 1][j];
+                cm.k[j] = kk(j);
+            }
+            cm.nk = i;
+            cm.dt_fixed = dt_fixed;
+            SBP_TRY_CUDA(combine_stages(s->d_blocks, s->d_inst, s->nblocks, prev, stage_in, cm, s->max_points, st));
+            in = stage_in;
+            ctime = T.c[i - 1];
+        }
+        SBP_TRY(launch_rhs(s, in, kk(i), ctime));
+    }
+    StageCombination cm{};
+    for (int j = 0; j < T.s; ++j) {
+        cm.coef[j] = T.b[j];
+        cm.k[j] = kk(j);
+    }
+    cm.nk = T.s;
+    cm.dt_fixed = dt_fixed;
+    SBP_TRY_CUDA(combine_stages(s->d_blocks, s->d_inst, s->nblocks, prev, fut ? fut : prev, cm, s->max_points, st));
+    if (fut2) {
+        for (int j = 0; j < T.s; ++j) cm.coef[j] = T.bstar[j];
+        SBP_TRY_CUDA(combine_stages(s->d_blocks, s->d_inst, s->nblocks, prev, fut2, cm, s->max_points, st));
+    }
+    return SBP_OK;
+}
 
 }  // namespace
 
@@ -1129,6 +1300,88 @@ sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q) {
     if (!sys || !d_q || !valid_block(sys, block)) return SBP_ERR_INVALID_ARGUMENT;
     *d_q = static_cast<char*>(sys->prev_hi) + sys->hb[block].q_off * sys->tsize();
     return SBP_OK;
+}
+
+sbp_status sbp_system_advance_tableau(sbp_system* sys, int tableau, int64_t nsteps) {
+    clear_error();
+    const Tableau* T = tableau_of(tableau);
+    if (!sys || !T || nsteps < 0) {
+        set_error("bad system, tableau %d or step count", tableau);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    if (sys->prec != 0) {
+        set_error("tableaus other than the fused RK4 run on f64 systems only");
+        return SBP_ERR_UNSUPPORTED;
+    }
+    cudaSetDevice(sys->device);
+    for (size_t i = 0; i < sys->active.size(); ++i)
+        if (!sys->active[i]) {
+            sys->active[i] = 1;
+            sys->sched_dirty = true;  // every instance takes part in the tableau steps
+        }
+    if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
+    SBP_TRY(ensure_kbuf(sys, T->s));
+    for (int64_t n = 0; n < nsteps; ++n) {
+        SBP_TRY(integrate_tableau(sys, *T, -1.0, nullptr, nullptr));
+        SBP_TRY_CUDA(time_update(sys->d_inst, sys->d_active, sys->ninst, sys->st()));
+    }
+    return check_status(sys);
+}
+
+sbp_status sbp_system_advance_adaptive(sbp_system* sys, double dt, double* guess_dt, double maxerr) {
+    clear_error();
+    if (!sys || !guess_dt || !(*guess_dt > 0.0) || !(dt >= 0.0)) {
+        set_error("bad system, dt or guess_dt");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    if (sys->prec != 0 || sys->nblocks != 1) {
+        set_error("advance_adaptive runs on single-block f64 systems (euler::System)");
+        return SBP_ERR_UNSUPPORTED;
+    }
+    for (int d = 0; d < 4; ++d)
+        if (sys->hb[0].bc_kind[d] != BC_THIS) {
+            set_error("advance_adaptive uses the own opposite edges on every side (This), as the reference");
+            return SBP_ERR_UNSUPPORTED;
+        }
+    cudaSetDevice(sys->device);
+    if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
+    const Tableau& T = *tableau_of(6);  // BogackiShampine
+    SBP_TRY(ensure_kbuf(sys, T.s));
+    cudaStream_t st = sys->st();
+    const BlockDev& B = sys->hb[0];
+    const int64_t n = (int64_t)B.nx * B.ny;
+    const double* hx = sys->hw + sys->hoff[0];
+    double* fut = static_cast<double*>(sys->uB);
+    double* fut2 = static_cast<double*>(sys->acc_hi);
+    double time = 0.0, guess = *guess_dt;
+    // euler::System::advance_adaptive (euler/src/lib.rs:149-186) as written: integrate advances
+    // `time` by the step, an accepted step adds the step once more; the error compared against
+    // maxerr is h2_err(prev, fut2).
+    for (int64_t iter = 0; time < dt; ++iter) {
+        if (iter > 100000000) {
+            set_error("advance_adaptive: no progress after %lld attempts", (long long)iter);
+            return SBP_ERR_NONPHYSICAL;
+        }
+        SBP_TRY(integrate_tableau(sys, T, guess, fut, fut2));
+        time += guess;
+        SBP_TRY_CUDA(pack_state(sys->d_blocks, 1, sys->d_poff4, 0, 0, fut2, nullptr, sys->staging, sys->max_points, st));
+        SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sizeof(double), st));
+        SBP_TRY_CUDA(diff_terms(sys->d_blocks, 0, sys->prev_hi, nullptr, static_cast<const double*>(sys->staging), hx,
+                                hx + B.nx, n, sys->d_sums, st));
+        double e2 = 0.0;
+        SBP_TRY_CUDA(cudaMemcpyAsync(&e2, sys->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));
+        SBP_TRY_CUDA(cudaStreamSynchronize(st));
+        const double err = std::sqrt(e2);
+        if (err < maxerr) {
+            time += guess;
+            SBP_TRY_CUDA(cudaMemcpyAsync(sys->prev_hi, fut, sys->nq * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            guess *= 1.05;
+        } else {
+            guess *= 0.8;
+        }
+    }
+    *guess_dt = guess;
+    return check_status(sys);
 }
 
 int sbp_system_group_count(sbp_system* sys) {

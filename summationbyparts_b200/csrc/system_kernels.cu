@@ -157,6 +157,23 @@ __global__ void max_speed_kernel(const BlockDev* __restrict__ blocks, int prec, 
     }
 }
 
+__global__ void combine_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst,
+                               const double* base, double* out, StageCombination cm) {
+    const BlockDev& B = blocks[blockIdx.y];
+    const double dt = cm.dt_fixed >= 0.0 ? cm.dt_fixed : inst[B.instance].dt;
+    double sc[kMaxStages];
+#pragma unroll
+    for (int j = 0; j < kMaxStages; ++j) sc[j] = cm.coef[j] * dt;  // (a * dt), then times k
+    const int64_t n4 = 4 * (int64_t)B.npad;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = B.q_off + i;
+        double v = base[g];
+        for (int j = 0; j < cm.nk; ++j)
+            if (cm.coef[j] != 0.0) v = v + sc[j] * cm.k[j][g];
+        out[g] = v;
+    }
+}
+
 __global__ void time_update_kernel(InstanceDev* inst, const int* __restrict__ active, int ninst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ninst && active[i]) inst[i].time = inst[i].time + inst[i].dt;
@@ -270,6 +287,12 @@ cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const 
 cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
                        int64_t max_points, unsigned long long* out2, cudaStream_t st) {
     max_speed_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, prec, q_hi, met64, out2);
+    return cudaGetLastError();
+}
+
+cudaError_t combine_stages(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const double* base,
+                           double* out, const StageCombination& cm, int64_t max_points, cudaStream_t st) {
+    combine_kernel<<<per_block_grid(nblocks, 4 * max_points), kT, 0, st>>>(blocks, inst, base, out, cm);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,20 @@ cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const 
 cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
                        int64_t max_points, unsigned long long* out2, cudaStream_t st);
 
+// One explicit Runge-Kutta combination (utils/integrate/src/lib.rs:193-211):
+// out = base; out = out + (coef[j] * dt) * k[j] for j = 0 .. nk-1 with coef[j] != 0, in that
+// order (Field::scaled_add, euler/src/lib.rs:205-212), dt = the block's instance dt or dt_fixed
+// when dt_fixed >= 0.  Over the padded planes of every block; out may be base.
+constexpr int kMaxStages = 8;
+struct StageCombination {
+    double coef[kMaxStages];
+    const double* k[kMaxStages];
+    int nk;
+    double dt_fixed;
+};
+cudaError_t combine_stages(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const double* base,
+                           double* out, const StageCombination& cm, int64_t max_points, cudaStream_t st);
+
 // time[i] += dt[i] for the instances whose flag is set.
 cudaError_t time_update(InstanceDev* inst, const int* active, int ninst, cudaStream_t st);
 

@@ -61,6 +61,13 @@ class System:
         self._sys.set_force_trad(False)
         self._sys.advance(nsteps)
 
+    def advance_adaptive(self, dt: float, guess_dt: float, maxerr: float) -> float:
+        """System::advance_adaptive (euler/src/lib.rs:149-186): embedded Bogacki-Shampine steps
+        with RHS_upwind until the local time reaches dt; returns the updated guess_dt (the
+        reference updates its `&mut guess_dt` argument)."""
+        self._sys.set_force_trad(False)
+        return self._sys.advance_adaptive(dt, guess_dt, maxerr)
+
     def field(self) -> np.ndarray:
         return self._sys.state(0)
 

@@ -207,6 +207,18 @@ class BlockSystem:
     def advance(self, nsteps: int) -> None:
         check(_capi.lib.sbp_system_advance(self.h, int(nsteps)))
 
+    def advance_tableau(self, tableau: str, nsteps: int) -> None:
+        """nsteps steps of integrate::<tableau> (rk4, rk4_38, euler, midpoint, rk6, fehlberg,
+        bogacki_shampine) with each instance's dt; f64 systems."""
+        check(_capi.lib.sbp_system_advance_tableau(self.h, _capi.TABLEAUS[tableau], int(nsteps)))
+
+    def advance_adaptive(self, dt: float, guess_dt: float, maxerr: float) -> float:
+        """euler::System::advance_adaptive on a single-block periodic (This) f64 system; returns
+        the updated guess_dt."""
+        g = ctypes.c_double(guess_dt)
+        check(_capi.lib.sbp_system_advance_adaptive(self.h, dt, ctypes.byref(g), maxerr))
+        return g.value
+
     def advance_instances(self, nsteps) -> None:
         arr = (ctypes.c_int64 * self.ninstances)(*[int(n) for n in nsteps])
         check(_capi.lib.sbp_system_advance_instances(self.h, arr))
