@@ -3,14 +3,18 @@
 // Compiled with -fmad=false: results are bit-identical to the reference's row path
 // (xi) and column path (eta) in the same dtype.
 //
-// Row direction: a CTA stages a row segment (plus halo) in shared memory with coalesced
-// loads; each thread then reads its window with 16-byte vector loads and produces
-// 16/sizeof(T) consecutive outputs (2 f64 or 4 f32), stored as one 16-byte vector.
-// Boundary-closure outputs (first/last M of the row) read global memory directly.
+// Row direction: a CTA stages kXiRows row segments (plus halo) in shared memory, with 16-byte
+// loads when the rows are 16-byte aligned; each thread
+// then reads its window with 16-byte vector loads and produces 16/sizeof(T) consecutive
+// outputs (2 f64 or 4 f32) per row, stored as one 16-byte vector.  Boundary-closure outputs
+// (first/last M of the row) read global memory directly.
 //
-// Column direction: one thread per column marches down a chunk of rows with the D-tap
-// window held in registers (fully unrolled ring, so no register moves), each load
-// coalesced across the warp; rows inside the boundary closures use the M x N blocks.
+// Column direction: one thread per 16 bytes of adjacent columns (2 f64 or 4 f32; one column
+// where the rows are not 16-byte aligned) marches down a chunk of rows with the D-tap windows
+// of its columns held in registers (fully unrolled ring, so no register moves), every row one
+// 16-byte load and one 16-byte store coalesced across the warp; rows inside the boundary
+// closures use the M x N blocks.  The reference's fused / unfused column split falls on a
+// multiple of 8 (f64) or 16 (f32) columns, so a thread's columns are all on the same side.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -23,7 +27,8 @@ namespace sbp {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kEtaRows = 128;
+constexpr int kEtaRows = 64;  // rows per column chunk: enough CTAs for even waves on 4096^2 fields
+constexpr int kXiRows = 1;
 
 template <class T>
 struct Vec;
@@ -45,32 +50,47 @@ __global__ void __launch_bounds__(kThreads)
     constexpr int PAD = ((H + K - 1) / K) * K;  // left/right halo, multiple of the vector width
     constexpr int SEG = kThreads * K;
     constexpr int NV = (K + 2 * PAD) / K;  // vectors in one thread's window
+    constexpr int BW = SEG + 2 * PAD;      // buffer width of one row
     using V = typename Vec<T>::type;
-    __shared__ __align__(16) T buf[SEG + 2 * PAD];
+    __shared__ __align__(16) T buf[kXiRows * BW];
 
     const int nseg = (nx + SEG - 1) / SEG;
-    const int64_t items = nbatch * (int64_t)ny * nseg;
+    const int nrg = (ny + kXiRows - 1) / kXiRows;
+    const int64_t items = nbatch * (int64_t)nrg * nseg;
     for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
         const int seg = (int)(it % nseg);
         const int64_t rr = it / nseg;
-        const int row = (int)(rr % ny);
-        const int64_t b = rr / ny;
-        const T* src = in + b * bstride + (int64_t)row * nx;
-        T* dst = out + b * bstride + (int64_t)row * nx;
+        const int row0 = (int)(rr % nrg) * kXiRows;
+        const int64_t b = rr / nrg;
+        const int nrows = min(kXiRows, ny - row0);
         const int s0 = seg * SEG;
-        const int base = s0 - PAD;  // column of buf[0]
+        const int base = s0 - PAD;  // column of buf[row][0]
         const int c_lo = base < 0 ? 0 : base;
         const int c_hi = min(nx, s0 + SEG + PAD);
-        for (int c = c_lo + threadIdx.x; c < c_hi; c += kThreads) buf[c - base] = __ldg(src + c);
+        // every load of the kXiRows rows is issued before the barrier
+        for (int r = 0; r < nrows; ++r) {
+            const T* src = in + b * bstride + (int64_t)(row0 + r) * nx;
+            T* bb = buf + r * BW;
+            if (vec_ok) {
+                // c_lo and c_hi are multiples of K (or nx, itself a multiple of K)
+                for (int c = c_lo + K * threadIdx.x; c < c_hi; c += K * kThreads)
+                    *reinterpret_cast<V*>(bb + c - base) = __ldg(reinterpret_cast<const V*>(src + c));
+            } else {
+                for (int c = c_lo + threadIdx.x; c < c_hi; c += kThreads) bb[c - base] = __ldg(src + c);
+            }
+        }
         __syncthreads();
 
         const int c0 = s0 + K * threadIdx.x;
-        if (c0 < nx) {
+        for (int r = 0; r < nrows && c0 < nx; ++r) {
+            const T* src = in + b * bstride + (int64_t)(row0 + r) * nx;
+            T* dst = out + b * bstride + (int64_t)(row0 + r) * nx;
+            const T* rbuf = buf + r * BW;
             T o[K];
             const bool interior = c0 >= M && c0 + K - 1 < nx - M;
             if (interior) {
                 T w[K + 2 * PAD];
-                const V* bv = reinterpret_cast<const V*>(buf + K * threadIdx.x);
+                const V* bv = reinterpret_cast<const V*>(rbuf + K * threadIdx.x);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) reinterpret_cast<V*>(w)[v] = bv[v];
                 // w[j] holds column c0 - PAD + j
@@ -145,6 +165,74 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// Column direction, K = 16 / sizeof(T) adjacent columns per thread (see the file comment).
+// Requires nx and bstride multiples of K and 16-byte aligned arrays.
+template <int OP, int KIND, class T>
+__global__ void __launch_bounds__(kThreads)
+    op_eta_vec_kernel(const T* __restrict__ in, T* __restrict__ out, int ny, int nx, int64_t nbatch, int64_t bstride,
+                      T idx, int simd) {
+    constexpr int M = OpShape<OP>::M, D = OpShape<OP>::D, H = OpShape<OP>::H;
+    constexpr int K = 16 / sizeof(T);
+    using V = typename Vec<T>::type;
+    const int ngroups = nx / K;
+    const int ncb = (ngroups + kThreads - 1) / kThreads;
+    const int nrc = (ny + kEtaRows - 1) / kEtaRows;
+    const int64_t items = nbatch * (int64_t)ncb * nrc;
+    for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const int cb = (int)(it % ncb);
+        const int64_t r1_ = it / ncb;
+        const int rc = (int)(r1_ % nrc);
+        const int64_t b = r1_ / nrc;
+        const int grp = cb * kThreads + threadIdx.x;
+        if (grp >= ngroups) continue;
+        const int col0 = grp * K;
+        const T* src = in + b * bstride + col0;
+        T* dst = out + b * bstride + col0;
+        const bool fused = col0 < simd;  // simd is a multiple of K: all K columns agree
+        const int y0 = rc * kEtaRows, y1 = min(ny, y0 + kEtaRows);
+        auto row_vec = [&](int r) { return __ldg(reinterpret_cast<const V*>(src + (int64_t)r * nx)); };
+        auto closure_row = [&](int r) {
+            T o[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                o[j] = sum_column<OP, KIND, T>(fused, r, ny, [&](int rr) { return __ldg(src + (int64_t)rr * nx + j); }) *
+                       idx;
+            *reinterpret_cast<V*>(dst + (int64_t)r * nx) = *reinterpret_cast<V*>(o);
+        };
+        for (int r = y0; r < y1 && r < M; ++r) closure_row(r);
+        for (int r = max(y0, ny - M); r < y1; ++r) closure_row(r);
+        const int i0 = max(y0, M), i1 = min(y1, ny - M);
+        if (i0 >= i1) continue;
+        V w[D];
+#pragma unroll
+        for (int k = 0; k < D - 1; ++k) w[k] = row_vec(i0 - H + k);
+        int r = i0;
+        for (; r + D <= i1; r += D) {
+#pragma unroll
+            for (int u = 0; u < D; ++u) {
+                w[(u + D - 1) % D] = row_vec(r + u + H);
+                T o[K];
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    T f = T(0);
+                    if (fused) {
+#pragma unroll
+                        for (int k = 0; k < D; ++k)
+                            f = fma_rn(reinterpret_cast<const T*>(&w[(u + k) % D])[j], Coef<OP, KIND, T>::diag(k), f);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < D; ++k)
+                            f = f + Coef<OP, KIND, T>::diag(k) * reinterpret_cast<const T*>(&w[(u + k) % D])[j];
+                    }
+                    o[j] = f * idx;
+                }
+                *reinterpret_cast<V*>(dst + (int64_t)(r + u) * nx) = *reinterpret_cast<V*>(o);
+            }
+        }
+        for (; r < i1; ++r) closure_row(r);
+    }
+}
+
 int g_num_sms = 0;
 
 int num_sms() {
@@ -160,21 +248,37 @@ int num_sms() {
 template <int OP, int KIND, class T>
 cudaError_t launch_t(int dir, const T* in, T* out, int64_t ny, int64_t nx, int64_t nbatch, int64_t bstride,
                      cudaStream_t st) {
-    const int blocks_cap = num_sms() * 8;
+    // One work item per CTA (the grid-stride loops only matter beyond this cap): the block
+    // scheduler then overlaps one CTA's loads with another's arithmetic, which the measured
+    // throughput prefers to a persistent grid that loops load -> compute -> store.
+    const int blocks_cap = 1 << 30;
+    (void)num_sms;
     if (dir == 0) {
         const T idx = inv_spacing<T>(OpShape<OP>::h2, nx);
         constexpr int K = 16 / sizeof(T);
         const int64_t nseg = (nx + kThreads * K - 1) / (kThreads * K);
-        const int64_t items = nbatch * ny * nseg;
+        const int64_t items = nbatch * ((ny + kXiRows - 1) / kXiRows) * nseg;
         const int grid = (int)(items < blocks_cap ? items : blocks_cap);
-        const bool vec_ok = (nx % K == 0) && (bstride % K == 0) && (reinterpret_cast<uintptr_t>(out) % 16 == 0);
+        const bool vec_ok = (nx % K == 0) && (bstride % K == 0) && (reinterpret_cast<uintptr_t>(out) % 16 == 0) &&
+                            (reinterpret_cast<uintptr_t>(in) % 16 == 0);
         op_xi_kernel<OP, KIND, T><<<grid, kThreads, 0, st>>>(in, out, (int)ny, (int)nx, nbatch, bstride, idx, vec_ok);
     } else {
         const T idx = inv_spacing<T>(OpShape<OP>::h2, ny);
         const int simd = (int)(simd_lanes<T>() * (nx / simd_lanes<T>()));
-        const int64_t items = nbatch * ((nx + kThreads - 1) / kThreads) * ((ny + kEtaRows - 1) / kEtaRows);
-        const int grid = (int)(items < blocks_cap ? items : blocks_cap);
-        op_eta_kernel<OP, KIND, T><<<grid, kThreads, 0, st>>>(in, out, (int)ny, (int)nx, nbatch, bstride, idx, simd);
+        constexpr int K = 16 / sizeof(T);
+        const bool vec_ok = (nx % K == 0) && (bstride % K == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) &&
+                            (reinterpret_cast<uintptr_t>(out) % 16 == 0);
+        if (vec_ok) {
+            const int64_t items = nbatch * ((nx / K + kThreads - 1) / kThreads) * ((ny + kEtaRows - 1) / kEtaRows);
+            const int grid = (int)(items < blocks_cap ? items : blocks_cap);
+            op_eta_vec_kernel<OP, KIND, T><<<grid, kThreads, 0, st>>>(in, out, (int)ny, (int)nx, nbatch, bstride, idx,
+                                                                      simd);
+        } else {
+            const int64_t items = nbatch * ((nx + kThreads - 1) / kThreads) * ((ny + kEtaRows - 1) / kEtaRows);
+            const int grid = (int)(items < blocks_cap ? items : blocks_cap);
+            op_eta_kernel<OP, KIND, T><<<grid, kThreads, 0, st>>>(in, out, (int)ny, (int)nx, nbatch, bstride, idx,
+                                                                  simd);
+        }
     }
     return cudaGetLastError();
 }
