@@ -28,11 +28,16 @@ METRIC = "Euler RK4 point-updates/s, 1 B200: batched FP32 vs plain FP64 at same 
 UNIT = "point-updates/s"
 # Algorithmic HBM bytes per point-update of the fused stage design (sum over the 4 stage
 # launches of the state, accumulator and metric planes each launch must read and write once).
-BYTES_PER_POINT_UPDATE = {"f32c": 464, "f64": 672}
-# The same per stage launch (stage 0..3): stage 0 reads the step-start state (and its low part)
-# and the metrics and writes the accumulator and the next stage input; stages 1 and 2 also read
-# the accumulator and the step-start state; stage 3 reads the accumulator and writes the new state.
-BYTES_PER_POINT_STAGE = {"f32c": (100, 132, 132, 100), "f64": (136, 200, 200, 136)}
+BYTES_PER_POINT_UPDATE = {"f32c": 384, "f64": 672}
+# The same per stage launch (stage 0..3).  f64: stage 0 reads the step-start state and the
+# metrics and writes the accumulator and the next stage input; stages 1 and 2 also read the
+# accumulator and the step-start state; stage 3 reads the accumulator and writes the new state.
+# f32c (state as a (hi, lo) f32 pair, the step's increment accumulated in one f32 array):
+# stage 0 reads the state's hi part and the metrics, writes the next stage input and the
+# increment; stages 1 and 2 read the stage input, metrics, increment and hi part and write the
+# next input and the increment; stage 3 reads the stage input, metrics, increment, hi and lo
+# parts and writes the new hi and lo parts.
+BYTES_PER_POINT_STAGE = {"f32c": (68, 100, 100, 116), "f64": (136, 200, 200, 136)}
 
 
 def parse():

@@ -30,8 +30,9 @@
 //
 // Precision: T = double reproduces the reference's f64 arithmetic operation by operation
 // (compile with -fmad=false).  T = float with COMP = true runs fluxes, dissipation and
-// stencils in f32 and keeps the RK4 state as a (hi, lo) f32 pair updated with TwoSum;
-// the SAT terms are computed in f64 from f64 metrics.
+// stencils in f32 and keeps the RK4 state as a (hi, lo) f32 pair; the step's increment
+// sum_j (b_j dt) k_j is accumulated in f32 and added to the pair once per step with TwoSum.
+// The SAT terms are computed in f64 from f64 metrics.
 #pragma once
 
 #include <type_traits>
@@ -57,8 +58,7 @@ struct StageArgs {
     const T* u_in;           // stage input state, all blocks
     const T* prev_hi;        // state at the start of the step
     const T* prev_lo;        // low part of the state (compensated precision only)
-    T* acc_hi;               // RK4 accumulator
-    T* acc_lo;
+    T* acc_hi;               // RK4 accumulator (compensated form: the step's f32 increment)
     T* u_out;                // next stage input (stages 0..2)
     T* new_hi;               // new state (stage 3)
     T* new_lo;
@@ -401,23 +401,24 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // The state arrays this stage's RK update reads (compensated form), in slot order:
-// stage 0: prev_lo, u_in (= prev_hi); stages 1, 2: acc_hi, acc_lo, prev_hi; stage 3: acc_hi, acc_lo.
+// stage 0: u_in (= prev_hi); stages 1, 2: delta (acc_hi), prev_hi; stage 3: delta, prev_hi, prev_lo.
 template <class T>
 __device__ __forceinline__ int stage_operands(const StageArgs<T>& A, const T* src[3]) {
     if (A.stage == 0) {
-        src[0] = A.prev_lo;
-        src[1] = A.u_in;
-        return 2;
+        src[0] = A.u_in;
+        return 1;
     }
     src[0] = A.acc_hi;
-    src[1] = A.acc_lo;
-    src[2] = A.prev_hi;
-    return A.stage < 3 ? 3 : 2;
+    src[1] = A.prev_hi;
+    src[2] = A.prev_lo;
+    return A.stage < 3 ? 2 : 3;
 }
 
 // Compensated RK update of one component at element e with its operands taken from the
 // staging slots (sop(a) = operand array a of this component at this point); same arithmetic
 // as rk_update.  cb, ca: this stage's B and A tableau entries times dt, already in f32.
+// The step's increment delta = sum_j (b_j dt) k_j is accumulated in f32 (acc_hi) and added to
+// the (hi, lo) state once, in stage 3, with TwoSum.
 template <class T, class SOP>
 __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, int64_t e, float cb, float ca, T kc, SOP sop) {
     if (A.stage == kStageK) {
@@ -426,24 +427,16 @@ __device__ __forceinline__ void rk_update_staged(const StageArgs<T>& A, int64_t 
     }
     const float kf = float(kc);
     if (A.stage == 0) {
-        float hi = float(sop(1));
-        float lo = float(sop(0));
-        A.u_out[e] = T(hi + ca * kf);
-        comp_add(hi, lo, __fmul_rn(cb, kf));
-        A.acc_hi[e] = T(hi);
-        A.acc_lo[e] = T(lo);
+        A.u_out[e] = T(float(sop(0)) + ca * kf);
+        A.acc_hi[e] = T(cb * kf);
     } else if (A.stage < 3) {
-        float hi = float(sop(0));
-        float lo = float(sop(1));
-        const float pv = float(sop(2));
-        A.u_out[e] = T(pv + ca * kf);
-        comp_add(hi, lo, __fmul_rn(cb, kf));
-        A.acc_hi[e] = T(hi);
-        A.acc_lo[e] = T(lo);
+        A.u_out[e] = T(float(sop(1)) + ca * kf);
+        A.acc_hi[e] = T(float(sop(0)) + cb * kf);
     } else {
-        float hi = float(sop(0));
-        float lo = float(sop(1));
-        comp_add(hi, lo, __fmul_rn(cb, kf));
+        const float d = float(sop(0)) + cb * kf;
+        float hi = float(sop(1));
+        float lo = float(sop(2));
+        comp_add(hi, lo, d);
         A.new_hi[e] = T(hi);
         A.new_lo[e] = T(lo);
     }
@@ -472,27 +465,21 @@ __device__ __forceinline__ void rk_update(const StageArgs<T>& A, int64_t e, T qv
             A.new_hi[e] = A.acc_hi[e] + cbt * kc;
         }
     } else {
+        // compensated form: see rk_update_staged
         const float cbf = float(cb);
         const float kf = float(kc);
         if (A.stage == 0) {
-            float hi = float(qv);
-            float lo = float(__ldg(A.prev_lo + e));
-            A.u_out[e] = T(hi + float(ca) * kf);
-            comp_add(hi, lo, __fmul_rn(cbf, kf));
-            A.acc_hi[e] = T(hi);
-            A.acc_lo[e] = T(lo);
+            A.u_out[e] = T(float(qv) + float(ca) * kf);
+            A.acc_hi[e] = T(cbf * kf);
         } else if (A.stage < 3) {
-            float hi = float(A.acc_hi[e]);
-            float lo = float(A.acc_lo[e]);
             const float pv = float(__ldg(A.prev_hi + e));
             A.u_out[e] = T(pv + float(ca) * kf);
-            comp_add(hi, lo, __fmul_rn(cbf, kf));
-            A.acc_hi[e] = T(hi);
-            A.acc_lo[e] = T(lo);
+            A.acc_hi[e] = T(float(A.acc_hi[e]) + cbf * kf);
         } else {
-            float hi = float(A.acc_hi[e]);
-            float lo = float(A.acc_lo[e]);
-            comp_add(hi, lo, __fmul_rn(cbf, kf));
+            const float d = float(A.acc_hi[e]) + cbf * kf;
+            float hi = float(A.prev_hi[e]);
+            float lo = float(A.prev_lo[e]);
+            comp_add(hi, lo, d);
             A.new_hi[e] = T(hi);
             A.new_lo[e] = T(lo);
         }

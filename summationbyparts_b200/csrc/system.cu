@@ -218,7 +218,6 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.prev_hi = prev;
     a.prev_lo = static_cast<const T*>(s->prev_lo);
     a.acc_hi = static_cast<T*>(s->acc_hi);
-    a.acc_lo = static_cast<T*>(s->acc_lo);
     a.new_hi = prev;
     a.new_lo = static_cast<T*>(s->prev_lo);
     a.met = s->prec == 0 ? reinterpret_cast<const T*>(s->met64) : reinterpret_cast<const T*>(s->met32);
@@ -800,7 +799,6 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc(&s->uB, s->nq * ts);
     if (precision == SBP_PRECISION_F32_COMPENSATED) {
         e = e ?: alloc(&s->prev_lo, s->nq * ts);
-        e = e ?: alloc(&s->acc_lo, s->nq * ts);
         e = e ?: alloc((void**)&s->met32, s->nm * sizeof(float));
     }
     e = e ?: alloc((void**)&s->met64, s->nm * sizeof(double));
@@ -825,7 +823,6 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: cudaMemsetAsync(s->uA, 0, s->nq * ts, st);
     e = e ?: cudaMemsetAsync(s->uB, 0, s->nq * ts, st);
     if (s->prev_lo) e = e ?: cudaMemsetAsync(s->prev_lo, 0, s->nq * ts, st);
-    if (s->acc_lo) e = e ?: cudaMemsetAsync(s->acc_lo, 0, s->nq * ts, st);
     e = e ?: cudaMemsetAsync(s->met64, 0, s->nm * sizeof(double), st);
     e = e ?: cudaMemsetAsync(s->status, 0, sizeof(unsigned), st);
     e = e ?: cudaMemsetAsync(s->d_zero, 0, sizeof(int64_t), st);
