@@ -1,12 +1,16 @@
 // Instantiations of the fused stage kernel: Upwind9/Upwind9h2 operator pairs, compensated f32 state.
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
+#include "stage_kernel_vec.cuh"
 
 namespace sbp {
 
-#define CASE(OX, OY, UPW, TYV)                                   \
-    if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
-        return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, TYV>);
+// 16-row tiles: stage_kernel; 32-row tiles: the 4-column micro-tile kernel.
+#define CASE(OX, OY, UPW, TYV)                                                        \
+    if (opx == OX && opy == OY && upw == UPW && ty == 16 && TYV == 16)                \
+        return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, 16>); \
+    if (opx == OX && opy == OY && upw == UPW && ty == kVecRows && TYV == kVecRows)    \
+        return reinterpret_cast<const void*>(&stage_kernel_vec<OX, OY, UPW>);
 
 const void* stage_ptr_f32_u9(int opx, int opy, bool upw, int ty) {
     CASE(UPWIND9, UPWIND9, true, 16)

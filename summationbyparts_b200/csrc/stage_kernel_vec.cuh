@@ -1,0 +1,372 @@
+// Fused RK4 stage kernel, compensated-f32 form, with 2 x 2 micro-tiles and paired f32 FMAs in
+// the stencil phase.
+//
+// Same right-hand side, same RK4 stage update and same edge-k hand-off as stage_kernel
+// (stage_kernel.cuh), with every output's sums taken in the same order, so the two kernels give
+// the same numbers.  What changes is the work decomposition of a 32 row x 32 column tile:
+//
+// * Phase 1 (pointwise fluxes and dissipation coefficients) is stage_kernel's, except where the
+//   values go in shared memory: the xi arrays are stored transposed ([column][row], row pitch
+//   kVecPitch = 34) with the even local columns first and the odd ones after them, the eta
+//   arrays row by row (pitch 32).
+// * Phase 2: thread (g, p) produces the 2 x 2 outputs of columns x0 + 2g, x0 + 2g + 1 and rows
+//   y0 + 2p, y0 + 2p + 1.  An xi tap is one 8-byte shared load carrying the two rows of one
+//   column (transposed layout); an eta tap one 8-byte load carrying the two columns of one row.
+//   Both feed __ffma2_rn, two f32 FMAs in one instruction: per output and stencil array
+//   (D + 1) / 4 loads and D / 2 paired FMAs in each direction, instead of D (xi) or
+//   (R + D - 1) / R (eta) loads and D FMAs.  A half-warp (g = lane & 15, one row pair) reads
+//   128 contiguous bytes of an eta row, or 16 consecutive column slots of the transposed xi
+//   array -- columns 2g + k share k's parity, so the even/odd split puts them in consecutive
+//   slots, and a slot pitch of 17 row pairs (odd) spreads them over all 16 bank pairs: both
+//   kinds of load are conflict-free.  Tiles that hold closure columns (rows) run the table
+//   path of stage_kernel for the xi (eta) sums, on every thread, so warps do not diverge.
+// * The RK operands (detJ and the stage's state arrays) are read from global memory into
+//   registers one component ahead of their use, which leaves the shared memory of two
+//   256-thread CTAs per SM to the stencil arrays.
+#pragma once
+
+#include "stage_kernel.cuh"
+
+namespace sbp {
+
+constexpr int kVecRows = 32;   // tile rows (256 threads = 16 column pairs x 16 row pairs)
+constexpr int kVecPitch = 34;  // row pitch of the transposed xi arrays: 17 row pairs
+
+template <int OPX, int OPY>
+struct VecGeom {
+    static constexpr int XC = region_extent(kTileX, OpShape<OPX>::H, OpShape<OPX>::M, OpShape<OPX>::N);
+    static constexpr int HYP = region_extent(kVecRows, OpShape<OPY>::H, OpShape<OPY>::M, OpShape<OPY>::N);
+    static constexpr int XCH = (XC + 1) / 2;   // column slots of each parity
+    static constexpr int XA = 2 * XCH * kVecPitch;  // elements of one (transposed) xi array
+    static constexpr int YA = HYP * kTileX;         // elements of one eta array
+};
+
+// Slot of local column c in a transposed xi array: even columns first, then the odd ones.
+template <int XCH>
+__device__ __forceinline__ int xslot(int c) { return (c >> 1) + (c & 1) * XCH; }
+
+__device__ __forceinline__ float2 ffma2(float2 a, float c, float2 acc) { return __ffma2_rn(a, make_float2(c, c), acc); }
+__device__ __forceinline__ float2 fmul2s(float2 a, float c) { return __fmul2_rn(a, make_float2(c, c)); }
+
+// Xi sums of one kind at columns c0, c0 + 1, each over the thread's two rows.  Local column
+// c0 - H + i of the transposed array, row r0, is at (i even ? pe : po) + (i / 2) * kVecPitch
+// (pe, po: the slots of columns c0 - H and c0 - H + 1; 8-byte aligned).  Interior columns: the
+// fma chain of stage_kernel's interior path.
+template <int OP, int KIND>
+__device__ __forceinline__ void xi_pair(const float* __restrict__ pe, const float* __restrict__ po, float idx,
+                                        float2 out[2]) {
+    constexpr int D = OpShape<OP>::D;
+    using C = Coef<OP, KIND, float>;
+    float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i <= D; ++i) {
+        const float2 v = *reinterpret_cast<const float2*>((i & 1 ? po : pe) + (i >> 1) * kVecPitch);
+        if (i < D) a0 = ffma2(v, C::diag(i), a0);
+        if (i >= 1) a1 = ffma2(v, C::diag(i - 1), a1);
+    }
+    out[0] = fmul2s(a0, idx);
+    out[1] = fmul2s(a1, idx);
+}
+
+// Eta sums of one kind at rows r0, r0 + 1, each over the thread's two columns: p points at the
+// eta array's row r0 - H, column c0 (8-byte aligned).
+template <int OP, int KIND>
+__device__ __forceinline__ void eta_pair(const float* __restrict__ p, float idx, float2 out[2]) {
+    constexpr int D = OpShape<OP>::D;
+    using C = Coef<OP, KIND, float>;
+    float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i <= D; ++i) {
+        const float2 v = *reinterpret_cast<const float2*>(p + i * kTileX);
+        if (i < D) a0 = ffma2(v, C::diag(i), a0);
+        if (i >= 1) a1 = ffma2(v, C::diag(i - 1), a1);
+    }
+    out[0] = fmul2s(a0, idx);
+    out[1] = fmul2s(a1, idx);
+}
+
+// Table row, first input and tap count of output i of a length-n line (closure or interior).
+template <int OP>
+__device__ __forceinline__ void table_row(int i, int n, int& row, int& base, int& ntaps) {
+    constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N, D = OpShape<OP>::D, H = OpShape<OP>::H;
+    if (i < M) {
+        row = i;
+        base = 0;
+        ntaps = N;
+    } else if (i >= n - M) {
+        row = M + i - (n - M);
+        base = n - N;
+        ntaps = N;
+    } else {
+        row = 2 * M;
+        base = i - H;
+        ntaps = D;
+    }
+}
+
+// Xi sum of one kind at column `col` of a closure tile over the thread's two rows, the table path
+// of stage_kernel (first product, then the fma chain): arr = transposed array at row r0.
+template <int OP, int KIND, int XCH>
+__device__ __forceinline__ float2 xi_table(const float* __restrict__ arr, int col, int nx, int lx0, float idx,
+                                           const float* __restrict__ ctab) {
+    constexpr int N = OpShape<OP>::N, NV = (N + 3) / 4;
+    int row, base, ntaps;
+    table_row<OP>(col, nx, row, base, ntaps);
+    const float* crow = ctab + coef_base(OP, KIND) + row * kCoefRow;
+    float cf[NV * 4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(cf + 4 * v) = __ldg(reinterpret_cast<const float4*>(crow) + v);
+    const float* pe = arr + xslot<XCH>(base - lx0) * kVecPitch;      // taps 0, 2, 4, ...
+    const float* po = arr + xslot<XCH>(base - lx0 + 1) * kVecPitch;  // taps 1, 3, 5, ...
+    float2 t = fmul2s(*reinterpret_cast<const float2*>(pe), cf[0]);
+#pragma unroll
+    for (int k = 1; k < N; ++k)
+        if (k < ntaps)
+            t = ffma2(*reinterpret_cast<const float2*>((k & 1 ? po : pe) + (k >> 1) * kVecPitch), cf[k], t);
+    return fmul2s(t, idx);
+}
+
+// Eta sum of one kind at row `row` of a closure tile over the thread's two columns, the table
+// path of stage_kernel (fma chain from zero): col = eta array at local row 0, column c0.
+template <int OP, int KIND>
+__device__ __forceinline__ float2 eta_table(const float* __restrict__ col, int row, int ny, int ly0, float idx,
+                                            const float* __restrict__ ctab) {
+    constexpr int N = OpShape<OP>::N;
+    int trow, base, ntaps;
+    table_row<OP>(row, ny, trow, base, ntaps);
+    const float* crow = ctab + coef_base(OP, KIND) + trow * kCoefRow;
+    const float* p = col + (base - ly0) * kTileX;
+    float2 t = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        if (k < ntaps) t = ffma2(*reinterpret_cast<const float2*>(p + k * kTileX), __ldg(crow + k), t);
+    return fmul2s(t, idx);
+}
+
+template <int OPX, int OPY>
+constexpr size_t vec_stage_smem(bool upw) {
+    using G = VecGeom<OPX, OPY>;
+    return sizeof(float) * (size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1);
+}
+
+template <int OPX, int OPY, bool UPW>
+__global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const StageArgs<float> A) {
+    using G = VecGeom<OPX, OPY>;
+    constexpr int TY = kVecRows;
+    constexpr int XA = G::XA, YA = G::YA, XCH = G::XCH;
+    constexpr int HX = OpShape<OPX>::H, HY = OpShape<OPY>::H;
+    constexpr int P1B = 4;  // phase-1 points per thread and batch
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sE = reinterpret_cast<float*>(smem_raw);  // [UPW ? 8 : 4][2 XCH][34]: Ehat, alpha_u q (transposed)
+    float* sF = sE + (UPW ? 8 : 4) * XA;             // [UPW ? 8 : 4][HYP][32]: Fhat, alpha_v q
+    const float gamma = float(A.gamma);
+    const int tid = threadIdx.x;
+    const int grp = tid & 15, rpr = tid >> 4;  // column pair, row pair (0..15 each)
+    unsigned bad = 0;
+    const float* src[3] = {nullptr, nullptr, nullptr};
+    const int nsrc = A.stage == kStageK ? 0 : stage_operands<float>(A, src);
+
+    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
+        const int4 td = A.tiles[t];
+        const BlockDev& B = A.blocks[td.x];
+        const int nx = B.nx, ny = B.ny;
+        const int64_t np = B.npad;
+        const int y0 = td.y, x0 = td.z;
+        const int y1 = min(y0 + TY, ny), x1 = min(x0 + kTileX, nx);
+        const int tw = x1 - x0, th = y1 - y0;
+        int lx0, lx1, ly0, ly1;
+        region_of<OPX>(x0, x1, nx, lx0, lx1);
+        region_of<OPY>(y0, y1, ny, ly0, ly1);
+        const int64_t qoff = B.q_off, eoff = B.e_off;
+        const float* q = A.u_in + qoff;
+        const float* mt = A.met + B.m_off;
+        const InstanceDev& I = A.inst[B.instance];
+        const float cbf = float(A.stage < 4 ? I.cb[A.stage] : 0.0);
+        const float caf = float(A.stage < 3 ? I.ca[A.stage] : 0.0);
+        const float idxx = B.idx_xi_f, idxy = B.idx_eta_f;
+
+        // ---------------- phase 1: pointwise quantities ----------------
+        // One index space over all threads: eta-region points (local rows 0 .. eh - 1, 32 slots per
+        // row, slots >= tw idle) followed by the xi-halo points (tile rows x hw columns, packed).
+        // A thread takes points p = tid, tid + 256, ... in batches of P1B, all loads of a batch
+        // issued before any of its points is evaluated.
+        const int eh = ly1 - ly0;
+        const int hl = x0 - lx0, hw = hl + (lx1 - x1);
+        const int n_eta = eh * kTileX, n_all = n_eta + th * hw;
+        const unsigned hw_inv = hw ? (65536u + hw - 1) / hw : 0u;  // exact floor(h / hw) for h < 1024
+        for (int pb = tid; pb < n_all; pb += P1B * kStageThreads) {
+            int pt[P1B], oxi[P1B], oeta[P1B];
+            float qv[P1B][4], m[P1B][4];
+#pragma unroll
+            for (int b = 0; b < P1B; ++b) {
+                const int p = pb + b * kStageThreads;
+                pt[b] = -1;
+                oxi[b] = -1;
+                oeta[b] = -1;
+                if (p < n_eta) {
+                    const int lr = p >> 5, tx = p & 31, row = ly0 + lr;
+                    if (tx < tw) {
+                        const int col = x0 + tx;
+                        pt[b] = row * nx + col;
+                        oeta[b] = lr * kTileX + tx;
+                        if (row >= y0 && row < y1) oxi[b] = xslot<XCH>(col - lx0) * kVecPitch + (row - y0);
+                    }
+                } else if (p < n_all) {
+                    const int h = p - n_eta;
+                    const int ty = (int)(((unsigned)h * hw_inv) >> 16);
+                    const int hc = h - ty * hw;
+                    const int col = hc < hl ? lx0 + hc : x1 + (hc - hl);
+                    pt[b] = (y0 + ty) * nx + col;
+                    oxi[b] = xslot<XCH>(col - lx0) * kVecPitch + ty;
+                }
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    qv[b][cc] = 1.0f;
+                    m[b][cc] = 0.0f;
+                }
+                if (pt[b] >= 0) {
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) qv[b][cc] = __ldg(q + cc * np + pt[b]);
+                    if (oxi[b] >= 0) {
+                        m[b][0] = __ldg(mt + np + pt[b]);
+                        m[b][1] = __ldg(mt + 2 * np + pt[b]);
+                    }
+                    if (oeta[b] >= 0) {
+                        m[b][2] = __ldg(mt + 3 * np + pt[b]);
+                        m[b][3] = __ldg(mt + 4 * np + pt[b]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < P1B; ++b)
+                if (pt[b] >= 0)
+                    pointwise<float, UPW, false>(qv[b], m[b], gamma, sE + (oxi[b] >= 0 ? oxi[b] : 0), XA,
+                                                 sF + (oeta[b] >= 0 ? oeta[b] : 0), YA, oxi[b] >= 0, oeta[b] >= 0,
+                                                 bad);
+        }
+
+        // Phase-2 operands of this thread (detJ and component 0's RK operands), loaded before
+        // the barrier so the loads overlap the other warps' phase 1.  Element of point (u, j)
+        // of component cc: e0 + cc * np + off[u][j].
+        const int c0 = x0 + 2 * grp, r0 = y0 + 2 * rpr;
+        const bool cok[2] = {2 * grp < tw, 2 * grp + 1 < tw};
+        const bool rok[2] = {2 * rpr < th, 2 * rpr + 1 < th};
+        const bool active = cok[0] && rok[0];
+        const int64_t e0 = qoff + (int64_t)r0 * nx + c0;
+        const int off[2][2] = {{0, 1}, {nx, nx + 1}};
+        float detj[2][2], opn[3][2][2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const bool ok = rok[u] && cok[j];
+                detj[u][j] = ok ? __ldg(mt + (e0 - qoff) + off[u][j]) : 1.0f;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(src[a] + e0 + off[u][j]) : 0.0f;
+            }
+        __syncthreads();
+
+        // ---------------- phase 2: stencils and stage update ----------------
+        if (active) {
+            const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
+            const bool eta_closure = y0 < OpShape<OPY>::M || y1 > ny - OpShape<OPY>::M;
+            const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
+            const float* xwe = xrow + xslot<XCH>(c0 - HX - lx0) * kVecPitch;      // ... column c0 - H
+            const float* xwo = xrow + xslot<XCH>(c0 - HX - lx0 + 1) * kVecPitch;  // ... column c0 - H + 1
+            const float* ecol = sF + (c0 - x0);                        // eta arrays at local row 0, column c0
+            const float* ewin = ecol + (r0 - HY - ly0) * kTileX;       // ... at row r0 - H
+            bool edge[2][2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    edge[u][j] = r0 + u == 0 || r0 + u == ny - 1 || c0 + j == 0 || c0 + j == nx - 1;
+            // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
+            float* out1 = A.stage == 3 ? A.new_hi : A.u_out;
+            float* out2 = A.stage == 3 ? A.new_lo : A.acc_hi;
+#pragma unroll 1
+            for (int cc = 0; cc < 4; ++cc) {
+                const int64_t ce = e0 + cc * np;
+                float nxt[3][2][2];
+                if (cc < 3) {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j)
+#pragma unroll
+                            for (int a = 0; a < 3; ++a)
+                                nxt[a][u][j] = (rok[u] && cok[j] && a < nsrc) ? __ldg(src[a] + ce + np + off[u][j]) : 0.0f;
+                }
+                // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
+                float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+                if (!xi_closure) {
+                    xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
+                    if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const int col = cok[j] ? c0 + j : c0;  // a column past the tile repeats c0
+                        ex[j] = xi_table<OPX, DIFF, XCH>(xrow + cc * XA, col, nx, lx0, idxx, A.coef);
+                        if constexpr (UPW)
+                            dx[j] = xi_table<OPX, DISS, XCH>(xrow + (4 + cc) * XA, col, nx, lx0, idxx, A.coef);
+                    }
+                }
+                // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
+                float2 ey[2], ay[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+                if (!eta_closure) {
+                    eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
+                    if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int row = rok[u] ? r0 + u : r0;  // a row past the tile repeats r0
+                        ey[u] = eta_table<OPY, DIFF>(ecol + cc * YA, row, ny, ly0, idxy, A.coef);
+                        if constexpr (UPW) ay[u] = eta_table<OPY, DISS>(ecol + (4 + cc) * YA, row, ny, ly0, idxy, A.coef);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        if (!(rok[u] && cok[j])) continue;
+                        const float exv = u == 0 ? ex[j].x : ex[j].y, dxv = u == 0 ? dx[j].x : dx[j].y;
+                        const float eyv = j == 0 ? ey[u].x : ey[u].y, ayv = j == 0 ? ay[u].x : ay[u].y;
+                        float kc;
+                        if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) / detj[u][j];
+                        else kc = (-exv - eyv) / detj[u][j];
+                        const int64_t e = ce + off[u][j];
+                        if (edge[u][j]) {
+                            const int row = r0 + u, col = c0 + j;
+                            A.kedge[4 * (eoff + edge_index(row, col, nx, ny)) + cc] = kc;
+                        } else if (A.stage == kStageK) {
+                            out1[e] = kc;
+                        } else if (A.stage == 0) {
+                            out1[e] = opn[0][u][j] + caf * kc;
+                            out2[e] = cbf * kc;
+                        } else if (A.stage < 3) {
+                            out1[e] = opn[1][u][j] + caf * kc;
+                            out2[e] = opn[0][u][j] + cbf * kc;
+                        } else {
+                            float hi = opn[1][u][j], lo = opn[2][u][j];
+                            comp_add(hi, lo, opn[0][u][j] + cbf * kc);
+                            out1[e] = hi;
+                            out2[e] = lo;
+                        }
+                    }
+                if (cc < 3) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int j = 0; j < 2; ++j) opn[a][u][j] = nxt[a][u][j];
+                }
+            }
+        }
+        // Every thread is done with this tile's shared arrays before the next tile's phase 1.
+        __syncthreads();
+    }
+    if (bad) atomicOr(A.status, bad);
+}
+
+}  // namespace sbp

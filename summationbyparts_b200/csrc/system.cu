@@ -21,6 +21,7 @@
 #include "sbp_ops.cuh"
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
+#include "stage_kernel_vec.cuh"
 #include "system_kernels.h"
 
 namespace sbp {
@@ -53,11 +54,20 @@ void region_host(int op, int a0, int a1, int n, int& lo, int& hi) {
 
 int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
 
-// Shared memory of one stage-kernel CTA (mirrors StageGeom in stage_kernel.cuh).
+// The compensated-f32 kernel of 32-row tiles is the 4-column micro-tile kernel (stage_kernel_vec).
+bool vec_kernel(int prec, int ty) { return prec == 1 && ty == kVecRows; }
+
+// Shared memory of one stage-kernel CTA (mirrors StageGeom in stage_kernel.cuh and VecGeom in
+// stage_kernel_vec.cuh).
 size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
     OpInfo ox, oy;
     op_info(opx, ox);
     op_info(opy, oy);
+    if (vec_kernel(prec, ty)) {
+        const int xc = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
+        const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
+        return sizeof(float) * (size_t)(4 * 2 * ((xc + 1) / 2) * kVecPitch + 4 * hyp * kTileX) * (upw ? 2 : 1);
+    }
     const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
     const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
     const size_t elems =
