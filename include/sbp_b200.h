@@ -173,7 +173,8 @@ sbp_status sbp_metrics_noalloc(int op_xi, int op_eta, const double* d_x, const d
 
 /* Build a system on `device`: copies the grids in, builds the f64 metrics on the device
  * (BaseSystem::create, multigrid/src/system.rs:55-78) and allocates state and stage buffers.
- * State starts at zero; instance dt starts at NaN and time at 0 (system.rs:126-128). */
+ * State starts at zero; instance dt starts at NaN and time at 0 (system.rs:126-128).
+ * A block has at most 2^28 points (larger grids return SBP_ERR_SHAPE). */
 sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nblocks, int ninstances,
                              int precision, double gamma, sbp_system** out);
 sbp_status sbp_system_destroy(sbp_system* sys);

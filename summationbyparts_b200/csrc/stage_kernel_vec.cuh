@@ -104,42 +104,49 @@ __device__ __forceinline__ void table_row(int i, int n, int& row, int& base, int
     }
 }
 
-// Xi sum of one kind at column `col` of a closure tile over the thread's two rows, the table path
-// of stage_kernel (first product, then the fma chain): arr = transposed array at row r0.
-template <int OP, int KIND, int XCH>
-__device__ __forceinline__ float2 xi_table(const float* __restrict__ arr, int col, int nx, int lx0, float idx,
+// Closure-tile descriptors of one output line (a column for xi, a row for eta), computed once
+// per tile: the coefficient row's offset in the operator's table part, the shared-memory
+// offsets of the first even and odd tap (xi: transposed slots; eta: rows, `eb`) and the tap
+// count (N for closure rows, D for interior ones).
+struct TableLine {
+    int crow, te, to, ntaps;
+};
+
+// Xi sum of one kind over the thread's two rows, table path of stage_kernel (first product, then
+// the fma chain): arr = transposed array at row r0.
+template <int OP, int KIND>
+__device__ __forceinline__ float2 xi_table(const float* __restrict__ arr, const TableLine& L, float idx,
                                            const float* __restrict__ ctab) {
     constexpr int N = OpShape<OP>::N, NV = (N + 3) / 4;
-    int row, base, ntaps;
-    table_row<OP>(col, nx, row, base, ntaps);
-    const float* crow = ctab + coef_base(OP, KIND) + row * kCoefRow;
+    const float* crow = ctab + coef_base(OP, KIND) + L.crow;
     float cf[NV * 4];
 #pragma unroll
     for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(cf + 4 * v) = __ldg(reinterpret_cast<const float4*>(crow) + v);
-    const float* pe = arr + xslot<XCH>(base - lx0) * kVecPitch;      // taps 0, 2, 4, ...
-    const float* po = arr + xslot<XCH>(base - lx0 + 1) * kVecPitch;  // taps 1, 3, 5, ...
+    const float* pe = arr + L.te;  // taps 0, 2, 4, ...
+    const float* po = arr + L.to;  // taps 1, 3, 5, ...
     float2 t = fmul2s(*reinterpret_cast<const float2*>(pe), cf[0]);
 #pragma unroll
     for (int k = 1; k < N; ++k)
-        if (k < ntaps)
+        if (k < L.ntaps)
             t = ffma2(*reinterpret_cast<const float2*>((k & 1 ? po : pe) + (k >> 1) * kVecPitch), cf[k], t);
     return fmul2s(t, idx);
 }
 
-// Eta sum of one kind at row `row` of a closure tile over the thread's two columns, the table
-// path of stage_kernel (fma chain from zero): col = eta array at local row 0, column c0.
+// Eta sum of one kind over the thread's two columns, table path of stage_kernel (fma chain from
+// zero): col = eta array at local row 0, column c0; the taps are rows L.te + k.
 template <int OP, int KIND>
-__device__ __forceinline__ float2 eta_table(const float* __restrict__ col, int row, int ny, int ly0, float idx,
+__device__ __forceinline__ float2 eta_table(const float* __restrict__ col, const TableLine& L, float idx,
                                             const float* __restrict__ ctab) {
-    constexpr int N = OpShape<OP>::N;
-    int trow, base, ntaps;
-    table_row<OP>(row, ny, trow, base, ntaps);
-    const float* crow = ctab + coef_base(OP, KIND) + trow * kCoefRow;
-    const float* p = col + (base - ly0) * kTileX;
+    constexpr int N = OpShape<OP>::N, NV = (N + 3) / 4;
+    const float* crow = ctab + coef_base(OP, KIND) + L.crow;
+    float cf[NV * 4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(cf + 4 * v) = __ldg(reinterpret_cast<const float4*>(crow) + v);
+    const float* p = col + L.te;
     float2 t = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < N; ++k)
-        if (k < ntaps) t = ffma2(*reinterpret_cast<const float2*>(p + k * kTileX), __ldg(crow + k), t);
+        if (k < L.ntaps) t = ffma2(*reinterpret_cast<const float2*>(p + k * kTileX), cf[k], t);
     return fmul2s(t, idx);
 }
 
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const int4 td = A.tiles[t];
         const BlockDev& B = A.blocks[td.x];
         const int nx = B.nx, ny = B.ny;
-        const int64_t np = B.npad;
+        const int np = (int)B.npad;  // in-block offsets fit 32 bits (checked when the system is built)
         const int y0 = td.y, x0 = td.z;
         const int y1 = min(y0 + TY, ny), x1 = min(x0 + kTileX, nx);
         const int tw = x1 - x0, th = y1 - y0;
@@ -247,22 +254,25 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 
         // Phase-2 operands of this thread (detJ and component 0's RK operands), loaded before
         // the barrier so the loads overlap the other warps' phase 1.  Element of point (u, j)
-        // of component cc: e0 + cc * np + off[u][j].
+        // of component cc: in-block offset e0 + cc * np + off[u][j] from the block bases.
         const int c0 = x0 + 2 * grp, r0 = y0 + 2 * rpr;
         const bool cok[2] = {2 * grp < tw, 2 * grp + 1 < tw};
         const bool rok[2] = {2 * rpr < th, 2 * rpr + 1 < th};
         const bool active = cok[0] && rok[0];
-        const int64_t e0 = qoff + (int64_t)r0 * nx + c0;
+        const int e0 = r0 * nx + c0;
         const int off[2][2] = {{0, 1}, {nx, nx + 1}};
+        const float* srcb[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) srcb[a] = a < nsrc ? src[a] + qoff : nullptr;
         float detj[2][2], opn[3][2][2];
 #pragma unroll
         for (int u = 0; u < 2; ++u)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const bool ok = rok[u] && cok[j];
-                detj[u][j] = ok ? __ldg(mt + (e0 - qoff) + off[u][j]) : 1.0f;
+                detj[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
 #pragma unroll
-                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(src[a] + e0 + off[u][j]) : 0.0f;
+                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
             }
         __syncthreads();
 
@@ -281,12 +291,31 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll
                 for (int j = 0; j < 2; ++j)
                     edge[u][j] = r0 + u == 0 || r0 + u == ny - 1 || c0 + j == 0 || c0 + j == nx - 1;
+            // table-path descriptors of the thread's columns (xi closure tiles) and rows (eta closure
+            // tiles); an output past the tile repeats the first one
+            TableLine xl[2], el[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                int trow, base;
+                table_row<OPX>(cok[j] ? c0 + j : c0, nx, trow, base, xl[j].ntaps);
+                xl[j].crow = trow * kCoefRow;
+                xl[j].te = xslot<XCH>(base - lx0) * kVecPitch;
+                xl[j].to = xslot<XCH>(base - lx0 + 1) * kVecPitch;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                int trow, base;
+                table_row<OPY>(rok[u] ? r0 + u : r0, ny, trow, base, el[u].ntaps);
+                el[u].crow = trow * kCoefRow;
+                el[u].te = (base - ly0) * kTileX;
+                el[u].to = 0;
+            }
             // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
-            float* out1 = A.stage == 3 ? A.new_hi : A.u_out;
-            float* out2 = A.stage == 3 ? A.new_lo : A.acc_hi;
+            float* out1 = (A.stage == 3 ? A.new_hi : A.u_out) + qoff;
+            float* out2 = (A.stage == 3 ? A.new_lo : A.acc_hi) + qoff;
 #pragma unroll 1
             for (int cc = 0; cc < 4; ++cc) {
-                const int64_t ce = e0 + cc * np;
+                const int ce = e0 + cc * np;
                 float nxt[3][2][2];
                 if (cc < 3) {
 #pragma unroll
@@ -295,7 +324,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         for (int j = 0; j < 2; ++j)
 #pragma unroll
                             for (int a = 0; a < 3; ++a)
-                                nxt[a][u][j] = (rok[u] && cok[j] && a < nsrc) ? __ldg(src[a] + ce + np + off[u][j]) : 0.0f;
+                                nxt[a][u][j] = (rok[u] && cok[j] && a < nsrc) ? __ldg(srcb[a] + (ce + np + off[u][j])) : 0.0f;
                 }
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
@@ -305,10 +334,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 } else {
 #pragma unroll
                     for (int j = 0; j < 2; ++j) {
-                        const int col = cok[j] ? c0 + j : c0;  // a column past the tile repeats c0
-                        ex[j] = xi_table<OPX, DIFF, XCH>(xrow + cc * XA, col, nx, lx0, idxx, A.coef);
-                        if constexpr (UPW)
-                            dx[j] = xi_table<OPX, DISS, XCH>(xrow + (4 + cc) * XA, col, nx, lx0, idxx, A.coef);
+                        ex[j] = xi_table<OPX, DIFF>(xrow + cc * XA, xl[j], idxx, A.coef);
+                        if constexpr (UPW) dx[j] = xi_table<OPX, DISS>(xrow + (4 + cc) * XA, xl[j], idxx, A.coef);
                     }
                 }
                 // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
@@ -319,9 +346,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 } else {
 #pragma unroll
                     for (int u = 0; u < 2; ++u) {
-                        const int row = rok[u] ? r0 + u : r0;  // a row past the tile repeats r0
-                        ey[u] = eta_table<OPY, DIFF>(ecol + cc * YA, row, ny, ly0, idxy, A.coef);
-                        if constexpr (UPW) ay[u] = eta_table<OPY, DISS>(ecol + (4 + cc) * YA, row, ny, ly0, idxy, A.coef);
+                        ey[u] = eta_table<OPY, DIFF>(ecol + cc * YA, el[u], idxy, A.coef);
+                        if constexpr (UPW) ay[u] = eta_table<OPY, DISS>(ecol + (4 + cc) * YA, el[u], idxy, A.coef);
                     }
                 }
 #pragma unroll
@@ -334,7 +360,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         float kc;
                         if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) / detj[u][j];
                         else kc = (-exv - eyv) / detj[u][j];
-                        const int64_t e = ce + off[u][j];
+                        const int e = ce + off[u][j];
                         if (edge[u][j]) {
                             const int row = r0 + u, col = c0 + j;
                             A.kedge[4 * (eoff + edge_index(row, col, nx, ny)) + cc] = kc;

@@ -54,6 +54,9 @@ void region_host(int op, int a0, int a1, int n, int& lo, int& hi) {
 
 int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
 
+// Largest block: 5 planes of pad64(points) elements stay below 2^31.
+constexpr int64_t kMaxBlockPoints = (int64_t)1 << 28;
+
 // The compensated-f32 kernel of 32-row tiles is the 4-column micro-tile kernel (stage_kernel_vec).
 bool vec_kernel(int prec, int ty) { return prec == 1 && ty == kVecRows; }
 
@@ -624,9 +627,15 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
             set_error("block %d: null grid", b);
             return SBP_ERR_INVALID_ARGUMENT;
         }
-        if (D.nx < 2 * ox.M || D.nx < ox.N || D.ny < 2 * oy.M || D.ny < oy.N || D.nx * D.ny > (int64_t)1 << 30) {
+        if (D.nx < 2 * ox.M || D.nx < ox.N || D.ny < 2 * oy.M || D.ny < oy.N) {
             set_error("block %d: %lld x %lld grid does not fit the operators (n >= max(2M, N))", b, (long long)D.ny,
                       (long long)D.nx);
+            return SBP_ERR_SHAPE;
+        }
+        // the stage kernels address a block's 5 metric planes with 32-bit offsets
+        if (D.nx * D.ny > kMaxBlockPoints) {
+            set_error("block %d: %lld x %lld grid has more than %lld points", b, (long long)D.ny, (long long)D.nx,
+                      (long long)kMaxBlockPoints);
             return SBP_ERR_SHAPE;
         }
         if (D.instance < 0 || D.instance >= ninstances) {
