@@ -757,7 +757,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
 // row, col).  Adds the SATs to the k the stage kernel stored and does the point's RK update.
 constexpr int kSatThreads = 128;
 template <class T, bool COMP>
-__global__ void __launch_bounds__(kSatThreads) sat_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
+__global__ void __launch_bounds__(kSatThreads, 4) sat_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
                                                           int nedges) {
     const int i = blockIdx.x * kSatThreads + threadIdx.x;
     if (i >= nedges) return;

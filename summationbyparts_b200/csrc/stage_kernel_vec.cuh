@@ -18,8 +18,9 @@
 //   128 contiguous bytes of an eta row, or 16 consecutive column slots of the transposed xi
 //   array -- columns 2g + k share k's parity, so the even/odd split puts them in consecutive
 //   slots, and a slot pitch of 17 row pairs (odd) spreads them over all 16 bank pairs: both
-//   kinds of load are conflict-free.  Tiles that hold closure columns (rows) run the table
-//   path of stage_kernel for the xi (eta) sums, on every thread, so warps do not diverge.
+//   kinds of load are conflict-free.  Tiles that hold closure columns run the table path of
+//   stage_kernel for the xi sums on every thread, so warps do not diverge; for the eta sums
+//   only the threads whose row pair holds a closure row take the table path.
 // * The RK operands (detJ and the stage's state arrays) are read from global memory into
 //   registers one component ahead of their use, which leaves the shared memory of two
 //   256-thread CTAs per SM to the stencil arrays.
@@ -279,7 +280,9 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         // ---------------- phase 2: stencils and stage update ----------------
         if (active) {
             const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
-            const bool eta_closure = y0 < OpShape<OPY>::M || y1 > ny - OpShape<OPY>::M;
+            // eta: the table path only for threads holding a closure row (warps of 4 rows, so
+            // at most one warp per block end diverges); their windows lie inside the region
+            const bool eta_closure = r0 < OpShape<OPY>::M || r0 + 1 >= ny - OpShape<OPY>::M;
             const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
             const float* xwe = xrow + xslot<XCH>(c0 - HX - lx0) * kVecPitch;      // ... column c0 - H
             const float* xwo = xrow + xslot<XCH>(c0 - HX - lx0 + 1) * kVecPitch;  // ... column c0 - H + 1
