@@ -163,7 +163,9 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     constexpr int TY = kVecRows;
     constexpr int XA = G::XA, YA = G::YA, XCH = G::XCH;
     constexpr int HX = OpShape<OPX>::H, HY = OpShape<OPY>::H;
-    constexpr int P1B = 4;  // phase-1 points per thread and batch
+    // phase-1 points per thread and batch: enough for an interior tile's whole region
+    // ((32 + 2 H_eta) rows x 32 + 32 rows x 2 H_xi points) in one batch of loads
+    constexpr int P1B = ((kVecRows + 2 * HY) * kTileX + kVecRows * 2 * HX + kStageThreads - 1) / kStageThreads;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sE = reinterpret_cast<float*>(smem_raw);  // [UPW ? 8 : 4][2 XCH][34]: Ehat, alpha_u q (transposed)
     float* sF = sE + (UPW ? 8 : 4) * XA;             // [UPW ? 8 : 4][HYP][32]: Fhat, alpha_v q
