@@ -338,33 +338,34 @@ def run_ours(args):
                 "speedup_f32_over_f64": value / v64}
 
     # end to end through the C ABI with host buffers: per step, upload the state from pinned host
-    # memory, advance one RK4 step, read the new state back (euler::System::advance_upwind + field())
+    # memory, advance one RK4 step, read the new state back (euler::System::advance_upwind + field()),
+    # as one sbp_system_advance_host call that pipelines the copies and the steps over chunks of
+    # instances
     e2e = None
     if not args.no_e2e:
         n = s32.state_count(0)
         host = torch.empty(n, dtype=torch.float64, pin_memory=True)
         s32.get_state_all(host)
         ke = max(3, min(args.steps, 10))
+        chunks = 0
         for _ in range(2):
-            s32.set_state_all(host)
-            s32.advance(1)
-            s32.get_state_all(host)
+            chunks = s32.advance_host(host, host, 1)
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(ke):
-            s32.set_state_all(host)
-            s32.advance(1)
-            s32.get_state_all(host)
+            s32.advance_host(host, host, 1)
         e1.record(stream)
         e1.synchronize()
         barrier()
         me = sharding.max_over_ranks(e0.elapsed_time(e1), dist if world > 1 else None)
         e2e = {"value": total_points * ke / (me / 1e3), "unit": UNIT, "h2d_bytes_per_step": n * 8,
-               "d2h_bytes_per_step": n * 8, "steps": ke,
-               "path": "sbp_system_set_state_all + sbp_system_advance(1) + sbp_system_get_state_all, f64 host state"}
+               "d2h_bytes_per_step": n * 8, "steps": ke, "chunks": chunks,
+               "path": "sbp_system_advance_host(q, q, 1): f64 host state in, one RK4 step, f64 host state out "
+                       "(= set_state_all + advance(1) + get_state_all), copies and steps pipelined over chunks "
+                       "of instances"}
 
     # per-kernel roofline of the stage kernels, with every instance active (the accuracy run
     # below re-initialises both systems)

@@ -200,6 +200,20 @@ sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q);
 /* The same packing into device memory (sbp_system_state_count(dtype) elements of 8 bytes for
  * SBP_F64, 4 for SBP_F32), for callers that keep the result on the GPU. */
 sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q);
+/* Host state in, `nsteps` RK4 steps, host state out: the result of sbp_system_set_state_all(q_in),
+ * sbp_system_advance(nsteps), sbp_system_get_state_all(q_out), bit for bit, in one call that
+ * pipelines the work over up to `nchunks` groups of whole instances (<= 0: 8): while one chunk's
+ * steps run, the next chunk's state is uploaded and the previous chunk's result downloaded, so
+ * the two PCIe directions and the GPU work overlap.  It replaces the reference's per-step
+ * `System::advance_upwind(dt)` + `System::field()` pair (euler/src/lib.rs:149-188) for callers
+ * whose state lives on the host.  q_in and q_out may be the same buffer; they should be pinned
+ * (page-locked) host memory for the copies to overlap.  Instances coupled to another instance
+ * (interfaces across instances, MultiGrid sides) run as one chunk.  The chunk step graphs are
+ * built on the first call and kept until the tile shape or the equation form changes. */
+sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in, void* q_out, int64_t nsteps,
+                                   int nchunks);
+/* Number of chunks the last sbp_system_advance_host call used (-1 for a null system). */
+int sbp_system_advance_host_chunks(sbp_system* sys);
 /* Number of state elements of sbp_system_{set,get}_state_all for dtype. */
 int64_t sbp_system_state_count(const sbp_system* sys, int dtype);
 

@@ -73,6 +73,8 @@ SIGNATURES = {
     "sbp_system_set_state_all": (_i, [_vp, _i, _vp]),
     "sbp_system_get_state_all": (_i, [_vp, _i, _vp]),
     "sbp_system_get_state_all_device": (_i, [_vp, _i, _vp]),
+    "sbp_system_advance_host": (_i, [_vp, _i, _vp, _vp, _i64, _i]),
+    "sbp_system_advance_host_chunks": (_i, [_vp]),
     "sbp_system_state_count": (_i64, [_vp, _i]),
     "sbp_system_set_dt": (_i, [_vp, _i, _d]),
     "sbp_system_set_time": (_i, [_vp, _i, _d]),

@@ -92,6 +92,19 @@ struct Group {
     int grid = 0;
 };
 
+// One chunk of sbp_system_advance_host: the blocks [b0, b1) (whole instances), their own step
+// graph and time-update mask, and the stream the chunk's copies and steps run on.
+struct Chunk {
+    int b0 = 0, b1 = 0;
+    std::vector<int> active;  // instances of the chunk
+    std::vector<Group> groups;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int* d_active = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
 }  // namespace
 }  // namespace sbp
 
@@ -147,6 +160,11 @@ struct sbp_system {
     cudaEvent_t ev_fork = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
+    // chunk schedules of sbp_system_advance_host, valid for the tile shape and form they were
+    // built with
+    std::vector<Chunk> chunks;
+    int chunk_ty = 0, chunk_req = 0;
+    bool chunk_trad = false;
 
     cudaStream_t st() const { return has_user_stream ? user_stream : stream; }
     size_t tsize() const { return prec == 0 ? sizeof(double) : sizeof(float); }
@@ -154,22 +172,37 @@ struct sbp_system {
 
 namespace {
 
-void free_groups(sbp_system* s) {
-    for (auto& g : s->groups) {
+void free_group_list(std::vector<Group>& groups, cudaGraph_t& graph, cudaGraphExec_t& gexec) {
+    for (auto& g : groups) {
         cudaFree(g.d_tiles);
         cudaFree(g.d_edges);
     }
-    s->groups.clear();
-    if (s->gexec) cudaGraphExecDestroy(s->gexec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    s->gexec = nullptr;
-    s->graph = nullptr;
+    groups.clear();
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+}
+
+void free_groups(sbp_system* s) { free_group_list(s->groups, s->graph, s->gexec); }
+
+void free_chunks(sbp_system* s) {
+    for (auto& c : s->chunks) {
+        if (c.st) cudaStreamSynchronize(c.st);
+        free_group_list(c.groups, c.graph, c.gexec);
+        if (c.d_active) cudaFree(c.d_active);
+        if (c.st) cudaStreamDestroy(c.st);
+        if (c.done) cudaEventDestroy(c.done);
+    }
+    s->chunks.clear();
+    s->chunk_req = 0;
 }
 
 void destroy_all(sbp_system* s) {
     if (!s) return;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    free_chunks(s);
     free_groups(s);
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
@@ -362,19 +395,22 @@ const Tableau* tableau_of(int id) {
     return id >= 0 && id < 7 ? &t[id] : nullptr;
 }
 
-// Build per-operator-pair tile lists for the active blocks, size shared memory and grids.
-sbp_status build_schedule(sbp_system* s) {
-    free_groups(s);
+// Build per-operator-pair tile lists for the blocks of the instances flagged in `active`, size
+// shared memory and grids, and capture one RK4 step (time update with the device mask
+// d_active) into a graph.
+sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const int* d_active,
+                            std::vector<Group>& groups, cudaGraph_t& graph_out, cudaGraphExec_t& gexec_out) {
+    free_group_list(groups, graph_out, gexec_out);
     const int TY = s->TY, TX = s->TX;
     for (int b = 0; b < s->nblocks; ++b) {
         const BlockDev& B = s->hb[b];
-        if (!s->active[B.instance]) continue;
+        if (!active[B.instance]) continue;
         OpInfo ox, oy;
         op_info(B.op_xi, ox);
         op_info(B.op_eta, oy);
         const bool upw = ox.upwind && oy.upwind && !s->force_trad;
         Group* gp = nullptr;
-        for (auto& g : s->groups)
+        for (auto& g : groups)
             if (g.opx == B.op_xi && g.opy == B.op_eta && g.upw == upw) gp = &g;
         if (!gp) {
             Group g;
@@ -386,22 +422,22 @@ sbp_status build_schedule(sbp_system* s) {
                 set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", B.op_xi, B.op_eta);
                 return SBP_ERR_UNSUPPORTED;
             }
-            s->groups.push_back(g);
-            gp = &s->groups.back();
+            groups.push_back(g);
+            gp = &groups.back();
         }
     }
-    std::vector<std::vector<int4>> tiles(s->groups.size()), edges(s->groups.size());
+    std::vector<std::vector<int4>> tiles(groups.size()), edges(groups.size());
     for (int b = 0; b < s->nblocks; ++b) {
         const BlockDev& B = s->hb[b];
-        if (!s->active[B.instance]) continue;
+        if (!active[B.instance]) continue;
         OpInfo ox, oy;
         op_info(B.op_xi, ox);
         op_info(B.op_eta, oy);
         const bool upw = ox.upwind && oy.upwind && !s->force_trad;
         size_t gi = 0;
-        for (; gi < s->groups.size(); ++gi)
-            if (s->groups[gi].opx == B.op_xi && s->groups[gi].opy == B.op_eta && s->groups[gi].upw == upw) break;
-        Group& g = s->groups[gi];
+        for (; gi < groups.size(); ++gi)
+            if (groups[gi].opx == B.op_xi && groups[gi].opy == B.op_eta && groups[gi].upw == upw) break;
+        Group& g = groups[gi];
         for (int y0 = 0; y0 < B.ny; y0 += TY)
             for (int x0 = 0; x0 < B.nx; x0 += TX) {
                 int lo, hi;
@@ -418,8 +454,8 @@ sbp_status build_schedule(sbp_system* s) {
         for (int r = 1; r < B.ny - 1; ++r) edges[gi].push_back(make_int4(b, r, 0, 0));
         for (int r = 1; r < B.ny - 1; ++r) edges[gi].push_back(make_int4(b, r, B.nx - 1, 0));
     }
-    for (size_t gi = 0; gi < s->groups.size(); ++gi) {
-        Group& g = s->groups[gi];
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        Group& g = groups[gi];
         g.ntiles = (int)tiles[gi].size();
         g.smem = stage_smem_host(s->prec, g.opx, g.opy, g.upw, TY);
         {
@@ -456,10 +492,8 @@ sbp_status build_schedule(sbp_system* s) {
                                          cudaMemcpyHostToDevice, s->stream));
         }
     }
-    std::vector<int> act(s->active);
-    SBP_TRY_CUDA(cudaMemcpyAsync(s->d_active, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
     SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
-    while (s->side.size() < s->groups.size()) {
+    while (s->side.size() < groups.size()) {
         cudaStream_t st;
         cudaEvent_t e;
         SBP_TRY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -471,19 +505,19 @@ sbp_status build_schedule(sbp_system* s) {
     SBP_TRY_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     sbp_status rc = SBP_OK;
     for (int stage = 0; stage < 4 && rc == SBP_OK; ++stage) {
-        if (s->groups.size() == 1) {
-            rc = launch_group(s, stage, s->groups[0], s->stream);
+        if (groups.size() == 1) {
+            rc = launch_group(s, stage, groups[0], s->stream);
         } else {
             cudaEventRecord(s->ev_fork, s->stream);
-            for (size_t gi = 0; gi < s->groups.size() && rc == SBP_OK; ++gi) {
+            for (size_t gi = 0; gi < groups.size() && rc == SBP_OK; ++gi) {
                 cudaStreamWaitEvent(s->side[gi], s->ev_fork, 0);
-                rc = launch_group(s, stage, s->groups[gi], s->side[gi]);
+                rc = launch_group(s, stage, groups[gi], s->side[gi]);
                 cudaEventRecord(s->ev[gi], s->side[gi]);
             }
-            for (size_t gi = 0; gi < s->groups.size(); ++gi) cudaStreamWaitEvent(s->stream, s->ev[gi], 0);
+            for (size_t gi = 0; gi < groups.size(); ++gi) cudaStreamWaitEvent(s->stream, s->ev[gi], 0);
         }
     }
-    if (rc == SBP_OK) rc = cuda_status(time_update(s->d_inst, s->d_active, s->ninst, s->stream), "time update");
+    if (rc == SBP_OK) rc = cuda_status(time_update(s->d_inst, d_active, s->ninst, s->stream), "time update");
     cudaGraph_t graph = nullptr;
     cudaError_t ee = cudaStreamEndCapture(s->stream, &graph);
     if (rc != SBP_OK) {
@@ -491,8 +525,16 @@ sbp_status build_schedule(sbp_system* s) {
         return rc;
     }
     SBP_TRY_CUDA(ee);
-    s->graph = graph;
-    SBP_TRY_CUDA(cudaGraphInstantiate(&s->gexec, graph, 0));
+    graph_out = graph;
+    SBP_TRY_CUDA(cudaGraphInstantiate(&gexec_out, graph, 0));
+    return SBP_OK;
+}
+
+// The system's own schedule: every active instance.
+sbp_status build_schedule(sbp_system* s) {
+    std::vector<int> act(s->active);
+    SBP_TRY_CUDA(cudaMemcpyAsync(s->d_active, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    SBP_TRY(build_step_graph(s, s->active, s->d_active, s->groups, s->graph, s->gexec));
     s->sched_dirty = false;
     return SBP_OK;
 }
@@ -1056,6 +1098,104 @@ sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
     return SBP_OK;
 }
+
+namespace {
+
+// Plan and build the chunks of sbp_system_advance_host: at most `want` contiguous block ranges
+// of whole instances with about equal points.  Instances coupled to another instance (a Grid or
+// Interpolate side naming a block of another instance, or any MultiGrid side) keep everything
+// in one chunk.
+sbp_status build_chunks(sbp_system* s, int want) {
+    free_chunks(s);
+    const int nb = s->nblocks;
+    bool coupled = false;
+    for (int b = 0; b < nb && !coupled; ++b)
+        for (int d = 0; d < 4; ++d) {
+            const BlockDev& B = s->hb[b];
+            if (B.bc_kind[d] == BC_MULTIGRID) coupled = true;
+            if ((B.bc_kind[d] == BC_GRID || B.bc_kind[d] == BC_INTERPOLATE) &&
+                s->hb[B.bc_nb[d]].instance != B.instance)
+                coupled = true;
+        }
+    // a cut before block b is allowed when no instance has blocks on both sides of it
+    std::vector<int> last(s->ninst, -1);
+    for (int b = 0; b < nb; ++b) last[s->hb[b].instance] = b;
+    std::vector<int> cuts = {0};
+    if (!coupled && want > 1) {
+        int64_t total = 0;
+        for (int b = 0; b < nb; ++b) total += (int64_t)s->hb[b].nx * s->hb[b].ny;
+        int reach = -1;
+        int64_t acc = 0;
+        for (int b = 0; b < nb; ++b) {
+            if (b > 0 && reach < b && acc >= total * (int64_t)cuts.size() / want && (int)cuts.size() < want)
+                cuts.push_back(b);
+            reach = std::max(reach, last[s->hb[b].instance]);
+            acc += (int64_t)s->hb[b].nx * s->hb[b].ny;
+        }
+    }
+    cuts.push_back(nb);
+    for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+        s->chunks.emplace_back();
+        Chunk& ch = s->chunks.back();
+        ch.b0 = cuts[c];
+        ch.b1 = cuts[c + 1];
+        ch.active.assign(s->ninst, 0);
+        for (int b = ch.b0; b < ch.b1; ++b) ch.active[s->hb[b].instance] = 1;
+        SBP_TRY_CUDA(cudaStreamCreateWithFlags(&ch.st, cudaStreamNonBlocking));
+        SBP_TRY_CUDA(cudaEventCreateWithFlags(&ch.done, cudaEventDisableTiming));
+        SBP_TRY_CUDA(cudaMalloc((void**)&ch.d_active, s->ninst * sizeof(int)));
+        SBP_TRY_CUDA(cudaMemcpyAsync(ch.d_active, ch.active.data(), s->ninst * sizeof(int), cudaMemcpyHostToDevice,
+                                     s->stream));
+        SBP_TRY(build_step_graph(s, ch.active, ch.d_active, ch.groups, ch.graph, ch.gexec));
+    }
+    s->chunk_ty = s->TY;
+    s->chunk_trad = s->force_trad;
+    s->chunk_req = want;
+    return SBP_OK;
+}
+
+}  // namespace
+
+sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in, void* q_out, int64_t nsteps,
+                                   int nchunks) {
+    clear_error();
+    if (!sys || !q_in || !q_out || nsteps < 0 || (dtype != SBP_F64 && dtype != SBP_F32))
+        return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    for (int i = 0; i < sys->ninst; ++i)
+        if (nsteps > 0 && !(sys->hi[i].dt == sys->hi[i].dt)) {
+            set_error("instance %d has no dt (call sbp_system_set_dt first)", i);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+    const int want = nchunks > 0 ? std::min(nchunks, 64) : 8;
+    if (sys->chunks.empty() || sys->chunk_req != want || sys->chunk_ty != sys->TY || sys->chunk_trad != sys->force_trad)
+        SBP_TRY(build_chunks(sys, want));
+    cudaStream_t st = sys->st();
+    const int64_t* poff = dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8;
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
+    SBP_TRY_CUDA(cudaEventRecord(sys->ev_fork, st));
+    const char* in = static_cast<const char*>(q_in);
+    char* out = static_cast<char*>(q_out);
+    char* stg = static_cast<char*>(sys->staging);
+    // every packed value takes 8 bytes (an f64, or an f32 hi and lo): block b starts at byte 8 dense_off[b]
+    for (Chunk& c : sys->chunks) {
+        const int64_t o0 = 8 * sys->dense_off[c.b0];
+        const int64_t o1 = c.b1 < sys->nblocks ? 8 * sys->dense_off[c.b1] : 8 * sys->dense_total;
+        SBP_TRY_CUDA(cudaStreamWaitEvent(c.st, sys->ev_fork, 0));
+        SBP_TRY_CUDA(cudaMemcpyAsync(stg + o0, in + o0, o1 - o0, cudaMemcpyHostToDevice, c.st));
+        SBP_TRY_CUDA(unpack_state(sys->d_blocks + c.b0, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->staging,
+                                  sys->prev_hi, sys->prev_lo, sys->max_points, c.st));
+        for (int64_t k = 0; k < nsteps; ++k) SBP_TRY_CUDA(cudaGraphLaunch(c.gexec, c.st));
+        SBP_TRY_CUDA(pack_state(sys->d_blocks + c.b0, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->prev_hi,
+                                sys->prev_lo, sys->staging, sys->max_points, c.st));
+        SBP_TRY_CUDA(cudaMemcpyAsync(out + o0, stg + o0, o1 - o0, cudaMemcpyDeviceToHost, c.st));
+        SBP_TRY_CUDA(cudaEventRecord(c.done, c.st));
+    }
+    for (Chunk& c : sys->chunks) SBP_TRY_CUDA(cudaStreamWaitEvent(st, c.done, 0));
+    return check_status(sys);
+}
+
+int sbp_system_advance_host_chunks(sbp_system* sys) { return sys ? (int)sys->chunks.size() : -1; }
 
 sbp_status sbp_system_set_dt(sbp_system* sys, int instance, double dt) {
     clear_error();

@@ -198,6 +198,16 @@ class BlockSystem:
         """Pack every block's state into device memory at d_ptr (state_count(dtype) elements)."""
         check(_capi.lib.sbp_system_get_state_all_device(self.h, dtype, ctypes.c_void_p(d_ptr)))
 
+    def advance_host(self, buf_in, buf_out, nsteps: int, dtype: int = F64, nchunks: int = 0) -> int:
+        """set_state_all(buf_in); advance(nsteps); get_state_all(buf_out) in one call, pipelined over
+        up to nchunks groups of whole instances (0: the library's default).  Returns the number of
+        chunks used.  Pinned host buffers let the copies overlap the steps."""
+        pi = buf_in.ctypes.data if isinstance(buf_in, np.ndarray) else buf_in.data_ptr()
+        po = buf_out.ctypes.data if isinstance(buf_out, np.ndarray) else buf_out.data_ptr()
+        check(_capi.lib.sbp_system_advance_host(self.h, dtype, ctypes.c_void_p(pi), ctypes.c_void_p(po), int(nsteps),
+                                                int(nchunks)))
+        return _capi.lib.sbp_system_advance_host_chunks(self.h)
+
     # -- stepping and diagnostics
     def max_dt(self, instance: int = 0) -> float:
         dt = ctypes.c_double()

@@ -169,3 +169,10 @@ def test_interpolate_rejects_bad_sizes():
     assert _capi.lib.sbp_interpolate(2, 1, _capi.F64, p, p, 21, 11, 1, 21, 11, None) == 2
     # unknown operator
     assert _capi.lib.sbp_interpolate(7, 1, _capi.F64, p, p, 41, 21, 1, 41, 21, None) == 1
+
+
+def test_advance_host_rejects_null_system():
+    from summationbyparts_b200 import _capi
+    p = ctypes.c_void_p(64)
+    assert _capi.lib.sbp_system_advance_host(None, _capi.F64, p, p, 1, 4) == 1
+    assert _capi.lib.sbp_system_advance_host_chunks(None) == -1
