@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--chunks", type=int, default=0,
+                   help="instance chunks of the end-to-end call (0: the library default)")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--tiles", default="", help="TY,TX,THREADS: fixed tile schedule instead of the autotuner")
@@ -349,14 +351,14 @@ def run_ours(args):
         ke = max(3, min(args.steps, 10))
         chunks = 0
         for _ in range(2):
-            chunks = s32.advance_host(host, host, 1)
+            chunks = s32.advance_host(host, host, 1, nchunks=args.chunks)
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(ke):
-            s32.advance_host(host, host, 1)
+            s32.advance_host(host, host, 1, nchunks=args.chunks)
         e1.record(stream)
         e1.synchronize()
         barrier()

@@ -202,7 +202,7 @@ sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q);
 sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q);
 /* Host state in, `nsteps` RK4 steps, host state out: the result of sbp_system_set_state_all(q_in),
  * sbp_system_advance(nsteps), sbp_system_get_state_all(q_out), bit for bit, in one call that
- * pipelines the work over up to `nchunks` groups of whole instances (<= 0: 8): while one chunk's
+ * pipelines the work over up to `nchunks` groups of whole instances (<= 0: 16): while one chunk's
  * steps run, the next chunk's state is uploaded and the previous chunk's result downloaded, so
  * the two PCIe directions and the GPU work overlap.  It replaces the reference's per-step
  * `System::advance_upwind(dt)` + `System::field()` pair (euler/src/lib.rs:149-188) for callers

@@ -1167,7 +1167,7 @@ sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in,
             set_error("instance %d has no dt (call sbp_system_set_dt first)", i);
             return SBP_ERR_INVALID_ARGUMENT;
         }
-    const int want = nchunks > 0 ? std::min(nchunks, 64) : 8;
+    const int want = nchunks > 0 ? std::min(nchunks, 64) : 16;
     if (sys->chunks.empty() || sys->chunk_req != want || sys->chunk_ty != sys->TY || sys->chunk_trad != sys->force_trad)
         SBP_TRY(build_chunks(sys, want));
     cudaStream_t st = sys->st();
