@@ -530,8 +530,13 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
     return SBP_OK;
 }
 
-// The system's own schedule: every active instance.
+// The system's own schedule: every active instance.  Steps of the previous schedule may still
+// be in flight on the system's stream (a caller's stream, see sbp_system_set_stream) and read the
+// time-update mask, so they finish before the mask changes.
 sbp_status build_schedule(sbp_system* s) {
+    SBP_TRY_CUDA(cudaStreamSynchronize(s->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+    free_groups(s);
     std::vector<int> act(s->active);
     SBP_TRY_CUDA(cudaMemcpyAsync(s->d_active, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, s->stream));
     SBP_TRY(build_step_graph(s, s->active, s->d_active, s->groups, s->graph, s->gexec));

@@ -268,3 +268,33 @@ def test_stage_launches_match_advance(precision):
         out.append(np.concatenate([g.state(b).ravel() for b in range(len(insts))]))
         g.close()
     assert out[0].tobytes() == out[1].tobytes()
+
+
+def test_ragged_steps_on_a_caller_stream():
+    """Ragged step counts on a caller's stream (sbp_system_set_stream): every instance ends at
+    time steps * dt, summed step by step as the device does, and the states equal those of the
+    same run on the system's own stream.  (The schedule changes between the ragged segments;
+    steps still in flight must not see the next segment's instance mask.)"""
+    from summationbyparts_b200 import workloads
+    from summationbyparts_b200.system import BlockSystem
+    insts = [i for i in workloads.ensemble_instances(40, seed=1) if i.side <= 90][:6]
+    steps = [3, 40, 7, 25, 1, 60]
+    out = []
+    for use_stream in (False, True):
+        g = BlockSystem(workloads.ensemble_blocks(insts), len(insts), "f32c", 1.4)
+        st = torch.cuda.Stream()
+        if use_stream:
+            g.set_stream(st.cuda_stream)
+        for k, inst in enumerate(insts):
+            g.set_vortex(inst.vortex, k)
+            g.set_dt(inst.dt, k)
+        g.init_vortex(0.0)
+        g.advance_instances(steps)
+        for k, inst in enumerate(insts):
+            t = 0.0
+            for _ in range(steps[k]):
+                t += inst.dt
+            assert g.time(k) == t, (k, g.time(k), t)
+        out.append(np.concatenate([g.state(b).ravel() for b in range(len(insts))]))
+        g.close()
+    assert out[0].tobytes() == out[1].tobytes()
