@@ -23,9 +23,10 @@ other coordinate, or 2-D (ny, nx)); missing fields come from the "default" grid.
 upwind4, upwind9, upwind4h2, upwind9h2, sbp4, sbp8.  Boundaries per side (north, south, east,
 west): "this", "vortex", {neighbour: name} (alias neighbor), {interpolate: {neighbour, operator:
 "4" | "8" | "9" | "9h2"}}, {multi: [{neighbour, start, end}, ...]}; an unspecified side takes the
-global boundary conditions ("initial_conditions", {vortex: ...} or "not_needed").  Initial and
-boundary conditions given as evalexpr expressions are not supported by this driver (they raise
-ConfigError).
+global boundary conditions ("initial_conditions", {vortex: ...} or "not_needed").  Initial
+conditions are a vortex or evalexpr expressions (summationbyparts_b200.expr, evaluated on the
+host); boundary conditions given as expressions (the reference's `Eval` boundaries) are not
+supported by this driver: a side that would need them raises ConfigError.
 """
 from __future__ import annotations
 
@@ -35,6 +36,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import multigrid as mg
+from .expr import Expressions, ExprError
 from .operators import SBP4, SBP8, Pair, Upwind4, Upwind4h2, Upwind9, Upwind9h2
 from .system import Vortice, VortexParameters
 
@@ -279,10 +281,16 @@ class Runtime:
     names: list
     grids: list                      # multigrid.Grid with boundary characteristics resolved
     integration_time: float
-    initial_vortex: VortexParameters
+    initial_vortex: VortexParameters | None   # vortex initial conditions, or
     boundary_vortex: VortexParameters | None
     gamma: float = 1.4
     raw: dict = field(default_factory=dict)
+    initial_expressions: Expressions | None = None  # expression initial conditions
+
+    @property
+    def initial(self):
+        """The initial conditions (and exact solution of --error): a vortex or expressions."""
+        return self.initial_expressions if self.initial_expressions is not None else self.initial_vortex
 
 
 def into_runtime(cfg: dict) -> Runtime:
@@ -291,20 +299,33 @@ def into_runtime(cfg: dict) -> Runtime:
     default = grids.pop("default", {}) or {}
     names = list(grids)
     index = {n: i for i, n in enumerate(names)}
+    gamma = float(cfg.get("gamma", 1.4))
     ic = cfg["initial_conditions"]
-    if not isinstance(ic, dict) or "vortex" not in ic:
-        raise ConfigError("only vortex initial conditions are supported (expressions need evalexpr)")
-    initial = _vortex(ic["vortex"])
+    initial, iexpr = None, None
+    if isinstance(ic, dict) and "vortex" in ic:
+        initial = _vortex(ic["vortex"])
+    elif isinstance(ic, dict) and "expressions" in ic:
+        try:
+            iexpr = Expressions.from_config(ic["expressions"], gamma)
+        except ExprError as e:
+            raise ConfigError(f"initial_conditions: {e}") from None
+    else:
+        raise ConfigError("initial_conditions must be a vortex or expressions")
+    # sides without their own boundary take the global boundary conditions; expression
+    # boundaries (BoundaryCharacteristic::Eval) are not available on this path
     gbc = cfg.get("boundary_conditions", "not_needed")
+    eval_bc = False
     if gbc == "initial_conditions":
         bvortex = initial
+        eval_bc = iexpr is not None
     elif gbc == "not_needed":
         bvortex = None
     elif isinstance(gbc, dict) and "vortex" in gbc:
         bvortex = _vortex(gbc["vortex"])
+    elif isinstance(gbc, dict) and "expressions" in gbc:
+        bvortex, eval_bc = None, True
     else:
-        raise ConfigError("only vortex boundary conditions are supported (expressions need evalexpr)")
-    gamma = float(cfg.get("gamma", 1.4))
+        raise ConfigError(f"unknown boundary_conditions {gbc!r}")
 
     def neighbour(n):
         if n not in index:
@@ -334,6 +355,9 @@ def into_runtime(cfg: dict) -> Runtime:
         for side in SIDES:
             bc = bcs.get(side, dbcs.get(side))
             if bc is None:
+                if eval_bc:
+                    raise ConfigError(f"grid {name!r}: expression boundary conditions are not supported by this "
+                                      "driver (give the side a boundary of its own)")
                 if bvortex is None:
                     raise ConfigError(f"Boundary conditions are not available, but needed for grid {name}")
                 sides.append(mg.VORTEX)
@@ -358,7 +382,7 @@ def into_runtime(cfg: dict) -> Runtime:
             else:
                 raise ConfigError(f"grid {name!r}: unknown boundary {bc!r}")
         out.append(mg.Grid(x, y, op, *sides, name=name))
-    return Runtime(names, out, float(cfg["integration_time"]), initial, bvortex, gamma, cfg)
+    return Runtime(names, out, float(cfg["integration_time"]), initial, bvortex, gamma, cfg, iexpr)
 
 
 def load(path: str) -> Runtime:

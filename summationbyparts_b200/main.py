@@ -97,8 +97,7 @@ def main(argv=None) -> int:
         return 0
     import torch
 
-    s = mg.System(rt.grids, rt.initial_vortex, rt.gamma, a.precision, a.device,
-                  boundary_vortex=rt.boundary_vortex)
+    s = mg.System(rt.grids, rt.initial, rt.gamma, a.precision, a.device, boundary_vortex=rt.boundary_vortex)
     dt = s.max_dt()
     s.set_dt(dt)
     ntime = int(round(rt.integration_time / dt))

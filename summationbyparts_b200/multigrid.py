@@ -64,20 +64,29 @@ def _bc(v):
 
 
 class System:
-    def __init__(self, grids: list[Grid], vortex: VortexParameters, gamma: float = 1.4, precision: str = "f64",
+    def __init__(self, grids: list[Grid], vortex, gamma: float = 1.4, precision: str = "f64",
                  device: int = 0, time: float = 0.0, boundary_vortex: VortexParameters | None = None):
-        """vortex: the initial conditions (and the exact solution of error()); boundary_vortex:
-        the vortex of VORTEX sides when it differs from the initial one."""
+        """vortex: the initial conditions (and the exact solution of error()), a
+        VortexParameters or an expr.Expressions (evaluated on the host at `time`, system.rs:135-153);
+        boundary_vortex: the vortex of VORTEX sides when it differs from the initial one."""
+        from .expr import Expressions
         specs = [BlockSpec(g.x, g.y, g.op, [_bc(g.north), _bc(g.south), _bc(g.east), _bc(g.west)], 0) for g in grids]
         self.grids = grids
-        self.vortex = vortex
-        self.boundary_vortex = boundary_vortex or vortex
+        self.expressions = vortex if isinstance(vortex, Expressions) else None
+        self.vortex = None if self.expressions is not None else vortex
+        self.boundary_vortex = boundary_vortex or self.vortex
         self._sys = BlockSystem(specs, 1, precision, gamma, device)
-        self._sys.set_vortex(vortex)
-        self._sys.init_vortex(time)
+        if self.expressions is not None:
+            for b, g in enumerate(grids):
+                self._sys.set_state(b, self.expressions.evaluate(time, g.x, g.y))
+            if self.boundary_vortex is not None:
+                self._sys.set_vortex(self.boundary_vortex)
+        else:
+            self._sys.set_vortex(vortex)
+            self._sys.init_vortex(time)
+            if self.boundary_vortex is not vortex:
+                self._sys.set_vortex(self.boundary_vortex)
         self._sys.set_time(time)
-        if self.boundary_vortex is not vortex:
-            self._sys.set_vortex(self.boundary_vortex)
 
     def max_dt(self) -> float:
         return self._sys.max_dt(0)
@@ -89,8 +98,12 @@ class System:
         self._sys.advance(nsteps)
 
     def error(self) -> float:
-        """Sum over blocks of h2_err against the initial-condition vortex at the current time
-        (multigrid/src/system.rs:618-635)."""
+        """Sum over blocks of h2_err against the initial conditions (vortex or expressions)
+        evaluated at the current time (multigrid/src/system.rs:618-635)."""
+        if self.expressions is not None:
+            t = self.time
+            return float(sum(self._sys.h2_err(b, self.expressions.evaluate(t, g.x, g.y))
+                             for b, g in enumerate(self.grids)))
         if self.boundary_vortex is not self.vortex:
             self._sys.set_vortex(self.vortex)
             e = float(self._sys.errors()[0])

@@ -69,9 +69,19 @@ def test_configuration_errors():
         rt(ops + ', a: { boundary_conditions: { north: { neighbour: "zz" } } }')
     with pytest.raises(config.ConfigError, match="not available"):
         rt(ops + ", a: {}", '"not_needed"')
-    with pytest.raises(config.ConfigError, match="expressions"):
-        config.into_runtime(config.loads(
-            '{grids: {a: {}}, integration_time: 1, initial_conditions: {expressions: {rho: "1", rhou: "1", rhov: "0", e: "2"}}}'))
+    # expression initial conditions are accepted; a side that falls back to expression boundary
+    # conditions (the reference's Eval boundaries) is not
+    expr_ic = '{expressions: {rho: "1", rhou: "1", rhov: "0", e: "2"}}'
+    r = config.into_runtime(config.loads('{grids: {' + ops + ', a: { boundary_conditions: { north: "this", '
+                                         'south: "this", east: "this", west: "this" } } }, integration_time: 1, '
+                                         'initial_conditions: ' + expr_ic + '}'))
+    assert r.initial_vortex is None and r.initial is r.initial_expressions
+    with pytest.raises(config.ConfigError, match="expression boundary"):
+        config.into_runtime(config.loads('{grids: {' + ops + ', a: {} }, integration_time: 1, initial_conditions: '
+                                         + expr_ic + ', boundary_conditions: "initial_conditions"}'))
+    with pytest.raises(config.ConfigError, match="initial_conditions"):
+        config.into_runtime(config.loads('{grids: {' + ops + ', a: {} }, integration_time: 1, initial_conditions: '
+                                         '{expressions: {rho: "1", u: "1"}}}'))
 
 
 def test_boundary_vortex_separate_from_initial():
