@@ -65,7 +65,8 @@ typedef enum sbp_boundary_kind {
     SBP_BC_GRID = 1,
     SBP_BC_VORTEX = 2,
     SBP_BC_INTERPOLATE = 3,
-    SBP_BC_MULTIGRID = 4
+    SBP_BC_MULTIGRID = 4,
+    SBP_BC_EVAL = 5
 } sbp_boundary_kind;
 
 /* sbp::operators::{Interpolation4, Interpolation8, Interpolation9, Interpolation9h2}
@@ -200,6 +201,22 @@ sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q);
 /* The same packing into device memory (sbp_system_state_count(dtype) elements of 8 bytes for
  * SBP_F64, 4 for SBP_F32), for callers that keep the result on the GPU. */
 sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q);
+/* Boundary data of SBP_BC_EVAL sides from expressions: BoundaryCharacteristic::Eval with the
+ * multigrid driver's evalexpr evaluator (euler/src/lib.rs:853-863, multigrid/src/eval/evalexpr.rs),
+ * evaluated on the device at every stage time for each edge point.  `form` SBP_EVAL_CONSERVATION
+ * gives programs for rho, rhou, rhov, e (rhou and rhov may read rho; e reads rho, rhou, rhov);
+ * SBP_EVAL_PRESSURE gives rho, u, v, p (u and v read rho; p reads rho, u, v), turned into the
+ * conserved state as euler/src/eval.rs:72-100 does.  Each program (len[k] <= 512 int32 words) is
+ * a stack program over f64: opcode words 1..23 of csrc/eval_program.cuh (EV_CONST k, EV_VAR v with
+ * v = x, y, t, rho, rhou, rhov, u, v, EV_LOAD / EV_STORE slot < 16, arithmetic, comparisons,
+ * logic, EV_SELECT, EV_FN1 / EV_FN2 function ids) with `nconsts` (<= 256) constants shared by
+ * the four programs; every program is checked (operands in range, stack depth <= 32, one value
+ * left) and rejected with SBP_ERR_INVALID_ARGUMENT otherwise.  summationbyparts_b200/expr.py
+ * compiles the expression text.  A system with SBP_BC_EVAL sides refuses to step until this has
+ * been called. */
+enum { SBP_EVAL_CONSERVATION = 0, SBP_EVAL_PRESSURE = 1 };
+sbp_status sbp_system_set_eval(sbp_system* sys, int form, const int32_t* const code[4], const int32_t len[4],
+                               const double* consts, int nconsts);
 /* Host state in, `nsteps` RK4 steps, host state out: the result of sbp_system_set_state_all(q_in),
  * sbp_system_advance(nsteps), sbp_system_get_state_all(q_out), bit for bit, in one call that
  * pipelines the work over up to `nchunks` groups of whole instances (<= 0: 16): while one chunk's

@@ -18,7 +18,8 @@ STATUS_NAMES = {0: "SBP_OK", 1: "SBP_ERR_INVALID_ARGUMENT", 2: "SBP_ERR_SHAPE", 
 
 F64, F32 = 0, 1
 PRECISION_F64, PRECISION_F32_COMPENSATED = 0, 1
-BC_THIS, BC_GRID, BC_VORTEX, BC_INTERPOLATE, BC_MULTIGRID = 0, 1, 2, 3, 4
+BC_THIS, BC_GRID, BC_VORTEX, BC_INTERPOLATE, BC_MULTIGRID, BC_EVAL = 0, 1, 2, 3, 4, 5
+EVAL_CONSERVATION, EVAL_PRESSURE = 0, 1
 INTERP4, INTERP8, INTERP9, INTERP9H2 = 0, 1, 2, 3
 TABLEAUS = {"rk4": 0, "rk4_38": 1, "euler": 2, "midpoint": 3, "rk6": 4, "fehlberg": 5, "bogacki_shampine": 6}
 NORTH, SOUTH, EAST, WEST = 0, 1, 2, 3
@@ -74,6 +75,7 @@ SIGNATURES = {
     "sbp_system_get_state_all": (_i, [_vp, _i, _vp]),
     "sbp_system_get_state_all_device": (_i, [_vp, _i, _vp]),
     "sbp_system_advance_host": (_i, [_vp, _i, _vp, _vp, _i64, _i]),
+    "sbp_system_set_eval": (_i, [_vp, _i, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(ctypes.c_int32), _dp, _i]),
     "sbp_system_advance_host_chunks": (_i, [_vp]),
     "sbp_system_state_count": (_i64, [_vp, _i]),
     "sbp_system_set_dt": (_i, [_vp, _i, _d]),

@@ -25,8 +25,9 @@ west): "this", "vortex", {neighbour: name} (alias neighbor), {interpolate: {neig
 "4" | "8" | "9" | "9h2"}}, {multi: [{neighbour, start, end}, ...]}; an unspecified side takes the
 global boundary conditions ("initial_conditions", {vortex: ...} or "not_needed").  Initial
 conditions are a vortex or evalexpr expressions (summationbyparts_b200.expr, evaluated on the
-host); boundary conditions given as expressions (the reference's `Eval` boundaries) are not
-supported by this driver: a side that would need them raises ConfigError.
+host); global boundary conditions given as expressions (or "initial_conditions" with expression
+initial conditions) make the unspecified sides the reference's `Eval` boundaries, evaluated on
+the device at every stage time.
 """
 from __future__ import annotations
 
@@ -36,7 +37,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import multigrid as mg
-from .expr import Expressions, ExprError
+from .expr import Expressions, ExprError, compile_program
 from .operators import SBP4, SBP8, Pair, Upwind4, Upwind4h2, Upwind9, Upwind9h2
 from .system import Vortice, VortexParameters
 
@@ -286,6 +287,7 @@ class Runtime:
     gamma: float = 1.4
     raw: dict = field(default_factory=dict)
     initial_expressions: Expressions | None = None  # expression initial conditions
+    boundary_expressions: Expressions | None = None  # data of EVAL sides
 
     @property
     def initial(self):
@@ -311,21 +313,30 @@ def into_runtime(cfg: dict) -> Runtime:
             raise ConfigError(f"initial_conditions: {e}") from None
     else:
         raise ConfigError("initial_conditions must be a vortex or expressions")
-    # sides without their own boundary take the global boundary conditions; expression
-    # boundaries (BoundaryCharacteristic::Eval) are not available on this path
+    # sides without their own boundary take the global boundary conditions: a vortex, or
+    # expressions (BoundaryCharacteristic::Eval, parsing.rs:55-70, 179-186)
     gbc = cfg.get("boundary_conditions", "not_needed")
-    eval_bc = False
+    bexpr = None
     if gbc == "initial_conditions":
         bvortex = initial
-        eval_bc = iexpr is not None
+        bexpr = iexpr
     elif gbc == "not_needed":
         bvortex = None
     elif isinstance(gbc, dict) and "vortex" in gbc:
         bvortex = _vortex(gbc["vortex"])
     elif isinstance(gbc, dict) and "expressions" in gbc:
-        bvortex, eval_bc = None, True
+        bvortex = None
+        try:
+            bexpr = Expressions.from_config(gbc["expressions"], gamma)
+        except ExprError as e:
+            raise ConfigError(f"boundary_conditions: {e}") from None
     else:
         raise ConfigError(f"unknown boundary_conditions {gbc!r}")
+    if bexpr is not None:
+        try:
+            compile_program(bexpr)  # every expression must run on the device
+        except ExprError as e:
+            raise ConfigError(f"boundary expressions: {e}") from None
 
     def neighbour(n):
         if n not in index:
@@ -355,9 +366,9 @@ def into_runtime(cfg: dict) -> Runtime:
         for side in SIDES:
             bc = bcs.get(side, dbcs.get(side))
             if bc is None:
-                if eval_bc:
-                    raise ConfigError(f"grid {name!r}: expression boundary conditions are not supported by this "
-                                      "driver (give the side a boundary of its own)")
+                if bexpr is not None:
+                    sides.append(mg.EVAL)
+                    continue
                 if bvortex is None:
                     raise ConfigError(f"Boundary conditions are not available, but needed for grid {name}")
                 sides.append(mg.VORTEX)
@@ -382,7 +393,7 @@ def into_runtime(cfg: dict) -> Runtime:
             else:
                 raise ConfigError(f"grid {name!r}: unknown boundary {bc!r}")
         out.append(mg.Grid(x, y, op, *sides, name=name))
-    return Runtime(names, out, float(cfg["integration_time"]), initial, bvortex, gamma, cfg, iexpr)
+    return Runtime(names, out, float(cfg["integration_time"]), initial, bvortex, gamma, cfg, iexpr, bexpr)
 
 
 def load(path: str) -> Runtime:

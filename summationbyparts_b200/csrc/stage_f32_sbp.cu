@@ -21,5 +21,6 @@ const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty) {
 }
 
 const void* sat_ptr_f32() { return reinterpret_cast<const void*>(&sat_kernel<float, true>); }
+const void* eval_ptr_f32() { return reinterpret_cast<const void*>(&eval_kernel<float>); }
 
 }  // namespace sbp

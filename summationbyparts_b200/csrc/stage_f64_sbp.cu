@@ -17,5 +17,6 @@ const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty) {
 }
 
 const void* sat_ptr_f64() { return reinterpret_cast<const void*>(&sat_kernel<double, false>); }
+const void* eval_ptr_f64() { return reinterpret_cast<const void*>(&eval_kernel<double>); }
 
 }  // namespace sbp

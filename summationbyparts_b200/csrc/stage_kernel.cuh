@@ -38,6 +38,7 @@
 #include <type_traits>
 
 #include "euler_device.cuh"
+#include "eval_program.cuh"
 #include "interp.cuh"
 #include "sbp_ops.cuh"
 
@@ -64,6 +65,8 @@ struct StageArgs {
     T* new_lo;
     T* kedge;                // k of block-edge points, 4 per point (edge_index order per block)
     const int4* mg;          // MultiGrid segments (block, start, end, -) of all block sides
+    const EvalDev* eval;     // expression programs of SBP_BC_EVAL sides
+    double* evz;             // SBP_BC_EVAL data of the launch's edge points (eval_kernel), 4 per point
     const T* met;            // metric planes in T
     const double* met64;     // metric planes in f64 (SAT terms)
     const double* xy;        // coordinates
@@ -497,7 +500,7 @@ __device__ __forceinline__ int opposite_edge_point(int d, int k, int gnx, int gn
 
 // SATs of one block-edge point in the reference's order N, S, E, W; k updated in place.
 template <class T>
-__device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int row,
+__device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int eidx, int row,
                                       int col, int pt, const double yv[4], double kv[4]) {
     const int nx = B.nx, ny = B.ny;
     const int64_t np = B.npad;
@@ -512,6 +515,11 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         if (kind == BC_VORTEX) {
             const double* xy = A.xy + B.x_off;
             vortex_point(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+        } else if (kind == BC_EVAL) {
+            // BoundaryCharacteristic::Eval (euler/src/lib.rs:853-863): the expressions at the stage
+            // time, evaluated for this edge point by eval_kernel just before
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) zv[cc] = A.evz[4 * (int64_t)eidx + cc];
         } else if (kind == BC_INTERPOLATE || kind == BC_MULTIGRID) {
             // boundary_extract (euler/src/lib.rs:816-846): data from neighbours' opposite edges
             const bool ns_ = d == NORTH || d == SOUTH;
@@ -778,9 +786,34 @@ __global__ void __launch_bounds__(kSatThreads, 4) sat_kernel(const StageArgs<T> 
         yv[cc] = double(q[cc * np + pt]);
         kv[cc] = double(A.kedge[slot + cc]);
     }
-    sat_edge<T>(A, I, B, row, col, pt, yv, kv);
+    sat_edge<T>(A, I, B, i, row, col, pt, yv, kv);
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, qoff + cc * np + pt, T(yv[cc]), T(kv[cc]), cb, ca);
+}
+
+// Expression boundary data (SBP_BC_EVAL sides) of a stage launch's edge points (edges[i] =
+// block, row, col) at the stage time, into evz[4 i ..]; launched before the edge kernel only for
+// systems with such sides, so the edge kernel itself stays free of the interpreter.
+template <class T>
+__global__ void __launch_bounds__(kSatThreads) eval_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
+                                                           int nedges) {
+    const int i = blockIdx.x * kSatThreads + threadIdx.x;
+    if (i >= nedges) return;
+    const int4 ed = edges[i];
+    const BlockDev& B = A.blocks[ed.x];
+    const int row = ed.y, col = ed.z;
+    const bool on[4] = {row == B.ny - 1, row == 0, col == B.nx - 1, col == 0};
+    bool any = false;
+    for (int d = 0; d < 4; ++d) any = any || (on[d] && B.bc_kind[d] == BC_EVAL);
+    if (!any) return;
+    const InstanceDev& I = A.inst[B.instance];
+    const double cst = A.stage == kStageK ? A.ctime : (A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5));
+    const double stime = cst == 0.0 ? I.time : I.time + I.dt * cst;
+    const int64_t pt = (int64_t)row * B.nx + col;
+    const double* xy = A.xy + B.x_off;
+    double z[4];
+    eval_state(*A.eval, A.gamma, stime, xy[pt], xy[B.npad + pt], z);
+    for (int cc = 0; cc < 4; ++cc) A.evz[4 * (int64_t)i + cc] = z[cc];
 }
 
 }  // namespace sbp

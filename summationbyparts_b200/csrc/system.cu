@@ -20,6 +20,7 @@
 #include "op_apply.h"
 #include "sbp_ops.cuh"
 #include "stage_dispatch.h"
+#include "eval_program.cuh"
 #include "stage_kernel.cuh"
 #include "stage_kernel_vec.cuh"
 #include "system_kernels.h"
@@ -86,6 +87,7 @@ struct Group {
     int ntiles = 0;
     int4* d_edges = nullptr;  // (block, row, col) of every edge point of the group's blocks
     int nedges = 0;
+    double* d_evz = nullptr;  // SBP_BC_EVAL data of those edge points (systems with such sides)
     int64_t points = 0;       // grid points of the group's blocks
     int WX = 0, HY = 0;
     size_t smem = 0;
@@ -145,6 +147,8 @@ struct sbp_system {
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
+    EvalDev* d_eval = nullptr;  // expression programs of SBP_BC_EVAL sides
+    bool has_eval = false, eval_set = false;
     double* kbuf = nullptr;  // k of the stages of a general tableau (kMaxStages x nq, f64), on demand
     int kbuf_stages = 0;
     // schedule
@@ -176,6 +180,7 @@ void free_group_list(std::vector<Group>& groups, cudaGraph_t& graph, cudaGraphEx
     for (auto& g : groups) {
         cudaFree(g.d_tiles);
         cudaFree(g.d_edges);
+        if (g.d_evz) cudaFree(g.d_evz);
     }
     groups.clear();
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -207,7 +212,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -272,6 +277,8 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.coef = static_cast<const T*>(s->d_coef);
     a.kedge = static_cast<T*>(s->kedge);
     a.mg = s->d_mg;
+    a.eval = s->d_eval;
+    a.evz = g.d_evz;
     a.gamma = s->gamma;
     a.status = s->status;
     return a;
@@ -284,17 +291,22 @@ sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t s
     const dim3 sat_grid((g.nedges + kSatThreads - 1) / kSatThreads);
     int4* edges = g.d_edges;
     int nedges = g.nedges;
+    const void* evk = s->prec == 0 ? eval_ptr_f64() : eval_ptr_f32();
     if (s->prec == 0) {
         StageArgs<double> a = stage_args<double>(s, stage, g);
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess && edges_too && s->has_eval)
+            e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
         if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     } else {
         StageArgs<float> a = stage_args<float>(s, stage, g);
         void* args[] = {&a};
         e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess && edges_too && s->has_eval)
+            e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
         if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     }
     return cuda_status(e, "stage kernel launch");
@@ -490,6 +502,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             SBP_TRY_CUDA(cudaMalloc(&g.d_edges, g.nedges * sizeof(int4)));
             SBP_TRY_CUDA(cudaMemcpyAsync(g.d_edges, edges[gi].data(), g.nedges * sizeof(int4),
                                          cudaMemcpyHostToDevice, s->stream));
+            if (s->has_eval) SBP_TRY_CUDA(cudaMalloc(&g.d_evz, (size_t)g.nedges * 4 * sizeof(double)));
         }
     }
     SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
@@ -555,7 +568,17 @@ sbp_status check_status(sbp_system* s) {
     return SBP_OK;
 }
 
+// Sides of kind SBP_BC_EVAL read the expression programs: they must be set before any step.
+sbp_status check_eval(const sbp_system* s) {
+    if (s->has_eval && !s->eval_set) {
+        set_error("the system has SBP_BC_EVAL sides: call sbp_system_set_eval first");
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    return SBP_OK;
+}
+
 sbp_status run_steps(sbp_system* s, int64_t n) {
+    SBP_TRY(check_eval(s));
     if (s->sched_dirty) SBP_TRY(build_schedule(s));
     for (int64_t i = 0; i < n; ++i) SBP_TRY_CUDA(cudaGraphLaunch(s->gexec, s->st()));
     return SBP_OK;
@@ -566,6 +589,7 @@ bool valid_block(const sbp_system* s, int b) { return b >= 0 && b < s->nblocks; 
 // k = RHS(u_in) (SATs included) into k_out for every group: the stage and edge kernels in their
 // k-only mode, SAT data at time + dt * ctime.
 sbp_status launch_rhs(sbp_system* s, const double* u_in, double* k_out, double ctime) {
+    SBP_TRY(check_eval(s));
     cudaStream_t st = s->st();
     for (const Group& g : s->groups) {
         if (g.ntiles == 0) continue;
@@ -579,6 +603,9 @@ sbp_status launch_rhs(sbp_system* s, const double* u_in, double* k_out, double c
         int4* edges = g.d_edges;
         int nedges = g.nedges;
         void* sargs[] = {&a, &edges, &nedges};
+        if (s->has_eval)
+            SBP_TRY_CUDA(cudaLaunchKernel(eval_ptr_f64(), dim3((g.nedges + kSatThreads - 1) / kSatThreads),
+                                          dim3(kSatThreads), sargs, 0, st));
         SBP_TRY_CUDA(cudaLaunchKernel(sat_ptr_f64(), dim3((g.nedges + kSatThreads - 1) / kSatThreads),
                                       dim3(kSatThreads), sargs, 0, st));
     }
@@ -692,7 +719,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         for (int d = 0; d < 4; ++d) {
             const int k = D.bc_kind[d];
             if (k != SBP_BC_THIS && k != SBP_BC_GRID && k != SBP_BC_VORTEX && k != SBP_BC_INTERPOLATE &&
-                k != SBP_BC_MULTIGRID) {
+                k != SBP_BC_MULTIGRID && k != SBP_BC_EVAL) {
                 set_error("block %d: unknown boundary kind %d", b, k);
                 return SBP_ERR_INVALID_ARGUMENT;
             }
@@ -813,6 +840,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         B.simd_f32 = (int)(16 * (D.nx / 16));
         for (int d = 0; d < 4; ++d) {
             B.bc_kind[d] = D.bc_kind[d];
+            if (D.bc_kind[d] == SBP_BC_EVAL) s->has_eval = true;
             B.bc_nb[d] = (D.bc_kind[d] == SBP_BC_GRID || D.bc_kind[d] == SBP_BC_INTERPOLATE) ? D.bc_neighbour[d] : b;
             if (D.bc_kind[d] == SBP_BC_INTERPOLATE) B.bc_aux[d] = D.bc_interp_op[d];
             if (D.bc_kind[d] == SBP_BC_MULTIGRID) {
@@ -882,6 +910,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
     e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
+    e = e ?: alloc((void**)&s->d_eval, sizeof(EvalDev));
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
     cudaStream_t st = s->stream;
     e = e ?: cudaMemsetAsync(s->prev_hi, 0, s->nq * ts, st);
@@ -1104,6 +1133,39 @@ sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q
     return SBP_OK;
 }
 
+sbp_status sbp_system_set_eval(sbp_system* sys, int form, const int32_t* const code[4], const int32_t len[4],
+                               const double* consts, int nconsts) {
+    clear_error();
+    if (!sys || !code || !len || (nconsts > 0 && !consts) || nconsts < 0) return SBP_ERR_INVALID_ARGUMENT;
+    if (form != EVAL_CONSERVATION && form != EVAL_PRESSURE) {
+        set_error("unknown expression form %d", form);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    if (nconsts > kEvalConsts) {
+        set_error("%d constants (at most %d)", nconsts, kEvalConsts);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
+    std::vector<EvalDev> h(1);
+    EvalDev& E = h[0];
+    std::memset(&E, 0, sizeof E);
+    E.form = form;
+    for (int k = 0; k < 4; ++k) {
+        if (!code[k]) return SBP_ERR_INVALID_ARGUMENT;
+        if (const char* why = eval_check(code[k], len[k], nconsts)) {
+            set_error("expression program %d: %s", k, why);
+            return SBP_ERR_INVALID_ARGUMENT;
+        }
+        E.len[k] = len[k];
+        std::memcpy(E.code[k], code[k], len[k] * sizeof(int32_t));
+    }
+    if (nconsts) std::memcpy(E.consts, consts, nconsts * sizeof(double));
+    cudaSetDevice(sys->device);
+    SBP_TRY_CUDA(cudaMemcpyAsync(sys->d_eval, &E, sizeof E, cudaMemcpyHostToDevice, sys->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(sys->st()));
+    sys->eval_set = true;
+    return SBP_OK;
+}
+
 namespace {
 
 // Plan and build the chunks of sbp_system_advance_host: at most `want` contiguous block ranges
@@ -1172,6 +1234,7 @@ sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in,
             set_error("instance %d has no dt (call sbp_system_set_dt first)", i);
             return SBP_ERR_INVALID_ARGUMENT;
         }
+    SBP_TRY(check_eval(sys));
     const int want = nchunks > 0 ? std::min(nchunks, 64) : 16;
     if (sys->chunks.empty() || sys->chunk_req != want || sys->chunk_ty != sys->TY || sys->chunk_trad != sys->force_trad)
         SBP_TRY(build_chunks(sys, want));
@@ -1557,6 +1620,7 @@ sbp_status sbp_system_group_info(sbp_system* sys, int group, int* op_xi, int* op
     clear_error();
     if (!sys) return SBP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(sys->device);
+    SBP_TRY(check_eval(sys));
     if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
     if (group < 0 || group >= (int)sys->groups.size()) {
         set_error("group %d out of range (%d groups)", group, (int)sys->groups.size());
@@ -1576,6 +1640,7 @@ sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int wi
         return SBP_ERR_INVALID_ARGUMENT;
     }
     cudaSetDevice(sys->device);
+    SBP_TRY(check_eval(sys));
     if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
     if (group < 0 || group >= (int)sys->groups.size()) {
         set_error("group %d out of range (%d groups)", group, (int)sys->groups.size());
@@ -1596,7 +1661,7 @@ int sbp_system_launches_per_step(const sbp_system* sys) {
         }
         return 8 * (int)pairs.size() + 1;
     }
-    return 8 * (int)sys->groups.size() + 1;
+    return (sys->has_eval ? 12 : 8) * (int)sys->groups.size() + 1;
 }
 
 }  // extern "C"

@@ -396,3 +396,227 @@ class Expressions:
                 rhou = u * rho
                 rhov = v * rho
         return np.stack([rho, rhou, rhov, e])
+
+
+# ----- programs for the device (SBP_BC_EVAL boundaries) --------------------------------------
+# Opcodes, variables and function ids of csrc/eval_program.cuh.
+(EV_CONST, EV_VAR, EV_LOAD, EV_STORE, EV_ADD, EV_SUB, EV_MUL, EV_DIV, EV_MOD, EV_POW, EV_NEG, EV_LT, EV_GT, EV_LE,
+ EV_GE, EV_EQ, EV_NE, EV_AND, EV_OR, EV_NOT, EV_SELECT, EV_FN1, EV_FN2) = range(1, 24)
+VARS = {"x": 0, "y": 1, "t": 2, "rho": 3, "rhou": 4, "rhov": 5, "u": 6, "v": 7}
+FN1 = {n: i for i, n in enumerate(["sin", "cos", "tan", "asin", "acos", "atan", "sinh", "cosh", "tanh", "asinh",
+                                   "acosh", "atanh", "exp", "exp2", "ln", "log2", "log10", "sqrt", "cbrt", "abs",
+                                   "floor", "ceil", "round"])}
+FN2 = {"pow": 0, "hypot": 1, "atan2": 2, "min": 3, "max": 4, "log": 5}
+_BINOP = {"+": EV_ADD, "-": EV_SUB, "*": EV_MUL, "/": EV_DIV, "%": EV_MOD, "^": EV_POW, "<": EV_LT, ">": EV_GT,
+          "<=": EV_LE, ">=": EV_GE, "==": EV_EQ, "!=": EV_NE, "&&": EV_AND, "||": EV_OR}
+_WITH_ARG = (EV_CONST, EV_VAR, EV_LOAD, EV_STORE, EV_FN1, EV_FN2)
+MAX_CODE, MAX_CONSTS, MAX_STACK, MAX_LOCALS = 512, 256, 32, 16
+_SINK = MAX_LOCALS - 1  # slot that swallows the value of a discarded sequence part
+
+
+class _Compiler:
+    """One field's expression -> a stack program.  A subtree without runtime variables is
+    evaluated here with the tree evaluator (exact integer semantics) and becomes a constant;
+    the rest runs in f64 on the device."""
+
+    def __init__(self, shared: dict, consts: list, runtime: tuple):
+        self.shared, self.consts, self.runtime = shared, consts, runtime
+        self.locals: dict = {}  # name -> ("const", value) or ("slot", index)
+        self.nslots = 0
+
+    def const_word(self, v) -> list:
+        v = float(v)
+        for k, c in enumerate(self.consts):
+            if c == v and math.copysign(1.0, c) == math.copysign(1.0, v):
+                return [EV_CONST, k]
+        self.consts.append(v)
+        return [EV_CONST, len(self.consts) - 1]
+
+    def words(self, r) -> list:
+        kind, v = r
+        if kind in ("none", "store"):
+            raise ExprError("an empty expression or an assignment where a number is needed")
+        if kind == "tuple":
+            raise ExprError("a tuple where a number is needed")
+        return self.const_word(v) if kind == "const" else list(v)
+
+    def comp(self, node):
+        kind = node[0]
+        if kind == "num":
+            return ("const", node[1])
+        if kind == "empty":
+            return ("none", None)
+        if kind == "var":
+            name = node[1]
+            if name in self.runtime:
+                return ("code", [EV_VAR, VARS[name]])
+            if name in self.locals:
+                k, v = self.locals[name]
+                return ("const", v) if k == "const" else ("code", [EV_LOAD, v])
+            if name in self.shared:
+                return ("const", self.shared[name])
+            raise ExprError(f"unknown variable {name}")
+        if kind == "assign":
+            r = self.comp(node[2])
+            if r[0] == "const":
+                self.locals[node[1]] = r
+                return ("none", None)
+            prev = self.locals.get(node[1])
+            if prev and prev[0] == "slot":
+                slot = prev[1]
+            else:
+                if self.nslots >= _SINK:
+                    raise ExprError("too many local variables")
+                slot = self.nslots
+                self.nslots += 1
+            code = self.words(r) + [EV_STORE, slot]
+            self.locals[node[1]] = ("slot", slot)
+            return ("store", code)
+        if kind == "seq":
+            a = self.comp(node[1])
+            b = self.comp(node[2])
+            if b[0] == "none":
+                return a
+            pre = a[1] if a[0] == "store" else (a[1] + [EV_STORE, _SINK] if a[0] == "code" else [])
+            if b[0] == "store":
+                return ("store", pre + b[1])
+            if not pre:
+                return b
+            return ("code", pre + self.words(b))
+        if kind == "tuple":
+            return ("tuple", [self.comp(n) for n in node[1]])
+        if kind == "un":
+            r = self.comp(node[2])
+            if r[0] == "const":
+                return ("const", evaluate(("un", node[1], ("num", r[1])), Context({})))
+            return ("code", self.words(r) + [EV_NEG if node[1] == "-" else EV_NOT])
+        if kind == "bin":
+            a, b = self.comp(node[2]), self.comp(node[3])
+            if a[0] == "const" and b[0] == "const":
+                return ("const", _py(_binary(node[1], a[1], b[1])))
+            return ("code", self.words(a) + self.words(b) + [_BINOP[node[1]]])
+        if kind == "call":
+            r = self.comp(node[2])
+            args = r[1] if r[0] == "tuple" else ([] if r[0] == "none" else [r])
+            if all(x[0] == "const" for x in args):
+                vals = tuple(x[1] for x in args)
+                return ("const", _py(_call(node[1], vals if len(vals) != 1 else vals[0])))
+            return ("code", self.call(node[1], args))
+        raise ExprError(f"bad node {kind}")
+
+    def call(self, name, args) -> list:
+        math_fn = name.startswith("math::")
+        f = name[6:] if math_fn else name
+        if math_fn and f in FN1 and f not in ("floor", "ceil", "round") and len(args) == 1:
+            return self.words(args[0]) + [EV_FN1, FN1[f]]
+        if not math_fn and f in ("floor", "ceil", "round") and len(args) == 1:
+            return self.words(args[0]) + [EV_FN1, FN1[f]]
+        if math_fn and f in ("pow", "hypot", "atan2", "log") and len(args) == 2:
+            return self.words(args[0]) + self.words(args[1]) + [EV_FN2, FN2[f]]
+        if not math_fn and f in ("min", "max") and args:
+            code = self.words(args[0])
+            for a in args[1:]:
+                code += self.words(a) + [EV_FN2, FN2[f]]
+            return code
+        if name == "if" and len(args) == 3:
+            return self.words(args[0]) + self.words(args[1]) + self.words(args[2]) + [EV_SELECT]
+        if name == "case" and len(args) % 2 == 1:
+            code = self.words(args[-1])
+            for k in range(len(args) - 3, -1, -2):
+                code = self.words(args[k]) + self.words(args[k + 1]) + code + [EV_SELECT]
+            return code
+        raise ExprError(f"function {name} with {len(args)} argument(s) cannot run on the device")
+
+
+def _depth(code: list) -> int:
+    sp = best = 0
+    pc = 0
+    while pc < len(code):
+        op = code[pc]
+        pc += 2 if op in _WITH_ARG else 1
+        if op in (EV_CONST, EV_VAR, EV_LOAD):
+            sp += 1
+        elif op in (EV_STORE, EV_FN2) or op in _BINOP.values():
+            sp -= 1
+        elif op == EV_SELECT:
+            sp -= 2
+        best = max(best, sp)
+    return best
+
+
+def compile_program(e: "Expressions"):
+    """The four device programs of an evaluator as sbp_system_set_eval takes them: (form: 0
+    conservation / 1 pressure, [code of each field], constants)."""
+    if e.form == "conservation":
+        names = ("rho", "rhou", "rhov", "e")
+        runtime = (("x", "y", "t"), ("x", "y", "t", "rho"), ("x", "y", "t", "rho"),
+                   ("x", "y", "t", "rho", "rhou", "rhov"))
+    else:
+        names = ("rho", "u", "v", "p")
+        runtime = (("x", "y", "t"), ("x", "y", "t", "rho"), ("x", "y", "t", "rho"), ("x", "y", "t", "rho", "u", "v"))
+    consts: list = []
+    codes = []
+    for name, rt in zip(names, runtime):
+        c = _Compiler(e._shared, consts, rt)
+        r = c.comp(e._trees[name])
+        if r[0] not in ("const", "code"):
+            raise ExprError(f"expression for {name} has no numeric value")
+        code = c.words(r)
+        if len(code) > MAX_CODE or _depth(code) > MAX_STACK:
+            raise ExprError(f"expression for {name} is too long for the device")
+        codes.append(code)
+    if len(consts) > MAX_CONSTS:
+        raise ExprError("too many constants for the device")
+    return (0 if e.form == "conservation" else 1), codes, consts
+
+
+def run_program(code: list, consts: list, vars_: dict):
+    """The device interpreter restated with numpy (test infrastructure for the compiler)."""
+    st, loc = [], {}
+    pc = 0
+    v = [vars_.get(n, 0.0) for n in VARS]
+    f1 = [np.sin, np.cos, np.tan, np.arcsin, np.arccos, np.arctan, np.sinh, np.cosh, np.tanh, np.arcsinh, np.arccosh,
+          np.arctanh, np.exp, np.exp2, np.log, np.log2, np.log10, np.sqrt, np.cbrt, np.abs, np.floor, np.ceil, _round]
+    f2 = [np.power, np.hypot, np.arctan2, np.fmin, np.fmax, lambda a, b: np.log(a) / np.log(b)]
+    ops = {EV_ADD: np.add, EV_SUB: np.subtract, EV_MUL: np.multiply, EV_DIV: np.divide, EV_MOD: np.fmod,
+           EV_POW: np.power}
+    cmp = {EV_LT: np.less, EV_GT: np.greater, EV_LE: np.less_equal, EV_GE: np.greater_equal, EV_EQ: np.equal,
+           EV_NE: np.not_equal}
+    with np.errstate(all="ignore"):
+        while pc < len(code):
+            op = code[pc]
+            arg = code[pc + 1] if op in _WITH_ARG else None
+            pc += 2 if op in _WITH_ARG else 1
+            if op == EV_CONST:
+                st.append(np.float64(consts[arg]))
+            elif op == EV_VAR:
+                st.append(v[arg])
+            elif op == EV_LOAD:
+                st.append(loc[arg])
+            elif op == EV_STORE:
+                loc[arg] = st.pop()
+            elif op == EV_NEG:
+                st.append(-st.pop())
+            elif op == EV_NOT:
+                st.append(np.where(st.pop() != 0.0, 0.0, 1.0))
+            elif op == EV_FN1:
+                st.append(f1[arg](st.pop()))
+            elif op == EV_FN2:
+                b = st.pop()
+                st.append(f2[arg](st.pop(), b))
+            elif op == EV_SELECT:
+                b, a, c = st.pop(), st.pop(), st.pop()
+                st.append(np.where(c != 0.0, a, b))
+            else:
+                b, a = st.pop(), st.pop()
+                if op in ops:
+                    st.append(ops[op](a, b))
+                elif op in cmp:
+                    st.append(np.where(cmp[op](a, b), 1.0, 0.0))
+                elif op == EV_AND:
+                    st.append(np.where((a != 0.0) & (b != 0.0), 1.0, 0.0))
+                else:
+                    st.append(np.where((a != 0.0) | (b != 0.0), 1.0, 0.0))
+    if len(st) != 1:
+        raise ExprError("program did not leave exactly one value")
+    return st[0]

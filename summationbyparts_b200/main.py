@@ -97,7 +97,8 @@ def main(argv=None) -> int:
         return 0
     import torch
 
-    s = mg.System(rt.grids, rt.initial, rt.gamma, a.precision, a.device, boundary_vortex=rt.boundary_vortex)
+    s = mg.System(rt.grids, rt.initial, rt.gamma, a.precision, a.device, boundary_vortex=rt.boundary_vortex,
+                  boundary_expressions=rt.boundary_expressions)
     dt = s.max_dt()
     s.set_dt(dt)
     ntime = int(round(rt.integration_time / dt))

@@ -18,11 +18,12 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._capi import BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX
+from ._capi import BC_EVAL, BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX
 from .system import BlockSpec, BlockSystem, VortexParameters
 
 THIS = "this"
 VORTEX = "vortex"
+EVAL = "eval"  # boundary data from the system's boundary expressions
 
 
 def grid_bc(g: int):
@@ -54,6 +55,8 @@ def _bc(v):
         return (BC_THIS, 0)
     if v == VORTEX:
         return (BC_VORTEX, 0)
+    if v == EVAL:
+        return (BC_EVAL, 0)
     if isinstance(v, tuple) and v[0] == "grid":
         return (BC_GRID, int(v[1]))
     if isinstance(v, tuple) and v[0] == "interpolate":
@@ -65,10 +68,13 @@ def _bc(v):
 
 class System:
     def __init__(self, grids: list[Grid], vortex, gamma: float = 1.4, precision: str = "f64",
-                 device: int = 0, time: float = 0.0, boundary_vortex: VortexParameters | None = None):
+                 device: int = 0, time: float = 0.0, boundary_vortex: VortexParameters | None = None,
+                 boundary_expressions=None):
         """vortex: the initial conditions (and the exact solution of error()), a
         VortexParameters or an expr.Expressions (evaluated on the host at `time`, system.rs:135-153);
-        boundary_vortex: the vortex of VORTEX sides when it differs from the initial one."""
+        boundary_vortex: the vortex of VORTEX sides when it differs from the initial one;
+        boundary_expressions: the expr.Expressions of EVAL sides (evaluated on the device at every
+        stage time)."""
         from .expr import Expressions
         specs = [BlockSpec(g.x, g.y, g.op, [_bc(g.north), _bc(g.south), _bc(g.east), _bc(g.west)], 0) for g in grids]
         self.grids = grids
@@ -86,6 +92,8 @@ class System:
             self._sys.init_vortex(time)
             if self.boundary_vortex is not vortex:
                 self._sys.set_vortex(self.boundary_vortex)
+        if boundary_expressions is not None:
+            self._sys.set_eval(boundary_expressions)
         self._sys.set_time(time)
 
     def max_dt(self) -> float:

@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi
-from ._capi import BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX, F32, F64, check  # noqa: F401
+from ._capi import BC_EVAL, BC_GRID, BC_INTERPOLATE, BC_MULTIGRID, BC_THIS, BC_VORTEX, F32, F64, check  # noqa: F401
 from .operators import SbpOperator2d
 
 PRECISIONS = {"f64": _capi.PRECISION_F64, "f32c": _capi.PRECISION_F32_COMPENSATED}
@@ -119,6 +119,18 @@ class BlockSystem:
     # -- configuration
     def set_force_trad(self, on: bool) -> None:
         check(_capi.lib.sbp_system_set_force_trad(self.h, int(on)))
+
+    def set_eval(self, expressions) -> None:
+        """Boundary data of BC_EVAL sides from an expr.Expressions evaluator, compiled to the
+        device programs of sbp_system_set_eval."""
+        from .expr import compile_program
+        form, codes, consts = compile_program(expressions)
+        arrs = [np.ascontiguousarray(np.array(c, dtype=np.int32)) for c in codes]
+        ptrs = (ctypes.POINTER(ctypes.c_int32) * 4)(*[a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) for a in arrs])
+        lens = (ctypes.c_int32 * 4)(*[len(c) for c in codes])
+        cv = np.ascontiguousarray(np.array(consts if consts else [0.0], dtype=np.float64))
+        check(_capi.lib.sbp_system_set_eval(self.h, form, ptrs, lens, cv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            len(consts)))
 
     def set_vortex(self, params: VortexParameters, instance: int = -1) -> None:
         vp = params.to_c()

@@ -69,16 +69,23 @@ def test_configuration_errors():
         rt(ops + ', a: { boundary_conditions: { north: { neighbour: "zz" } } }')
     with pytest.raises(config.ConfigError, match="not available"):
         rt(ops + ", a: {}", '"not_needed"')
-    # expression initial conditions are accepted; a side that falls back to expression boundary
-    # conditions (the reference's Eval boundaries) is not
+    # expression initial conditions; sides without their own boundary take expression (Eval)
+    # boundaries from "initial_conditions" or from boundary expressions
     expr_ic = '{expressions: {rho: "1", rhou: "1", rhov: "0", e: "2"}}'
     r = config.into_runtime(config.loads('{grids: {' + ops + ', a: { boundary_conditions: { north: "this", '
                                          'south: "this", east: "this", west: "this" } } }, integration_time: 1, '
                                          'initial_conditions: ' + expr_ic + '}'))
-    assert r.initial_vortex is None and r.initial is r.initial_expressions
-    with pytest.raises(config.ConfigError, match="expression boundary"):
+    assert r.initial_vortex is None and r.initial is r.initial_expressions and r.boundary_expressions is None
+    r = config.into_runtime(config.loads('{grids: {' + ops + ', a: { boundary_conditions: { north: "this" } } }, '
+                                         'integration_time: 1, initial_conditions: ' + expr_ic
+                                         + ', boundary_conditions: "initial_conditions"}'))
+    a = r.grids[0]
+    assert a.north == mg.THIS and a.south == a.east == a.west == mg.EVAL
+    assert r.boundary_expressions is r.initial_expressions
+    with pytest.raises(config.ConfigError, match="boundary expressions"):
         config.into_runtime(config.loads('{grids: {' + ops + ', a: {} }, integration_time: 1, initial_conditions: '
-                                         + expr_ic + ', boundary_conditions: "initial_conditions"}'))
+                                         + expr_ic + ', boundary_conditions: {expressions: {rho: "1", rhou: '
+                                         '"math::nosuch(x)", rhov: "0", e: "2"}}}'))
     with pytest.raises(config.ConfigError, match="initial_conditions"):
         config.into_runtime(config.loads('{grids: {' + ops + ', a: {} }, integration_time: 1, initial_conditions: '
                                          '{expressions: {rho: "1", u: "1"}}}'))

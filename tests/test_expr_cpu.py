@@ -105,3 +105,60 @@ def test_scalar_results_fill_the_grid():
     x, y = grid()
     q = e.evaluate(0.0, x, y)
     assert q.shape == (4,) + x.shape and np.all(q[0] == 1.0) and np.all(q[3] == 1.0 / (1.4 - 1.0))
+
+
+PROGRAM_CASES = [
+    ({"globals": "M = 0.4; p0 = 1/(GAMMA * M^2);", "rho": "1",
+      "u": "r = math::hypot(x, y); -math::sin(math::atan2(y, x)) * case(r < 0.2, 5*r, r < 0.4, 2 - 5*r, 0)",
+      "v": "r = math::hypot(x, y); math::cos(math::atan2(y, x)) * case(r < 0.2, 5*r, r < 0.4, 2 - 5*r, 0)",
+      "p": "r = math::hypot(x, y); case(r < 0.2, p0 + 25.0/2.0*r*r, p0 - 2 + 4*math::ln(2) + r)"}, 5.0 / 3.0),
+    ({"globals": "ua = 1; va = 1; b = 5; Tf = (GAMMA - 1)*b*b/(8*GAMMA*PI*PI)",
+      "rho": "x0 = ua*t; y0 = va*t; math::pow(1 - Tf*math::exp(1 - ((x - x0)*(x - x0) + (y - y0)*(y - y0))), 1.0/(GAMMA - 1))",
+      "u": "x0 = ua*t; y0 = va*t; ua + b/(2*PI) * math::exp((1 - ((x - x0)^2 + (y - y0)^2))/2)*(-(y - y0))",
+      "v": "x0 = ua*t; y0 = va*t; va + b/(2*PI) * math::exp((1 - ((x - x0)^2 + (y - y0)^2))/2)*(x - x0)",
+      "p": "math::pow(rho, GAMMA)"}, 1.4),
+    ({"rho": "2 + 0.1*math::cos(x) + if(y > 0.5, 0.05, -0.05)", "rhou": "rho * max(x, 0.3, y)",
+      "rhov": "-rho * min(1, y)", "e": "10 + rhou*rhou/rho + floor(3.7) - 7 / 2 + 7 % 3 + round(x)"}, 1.4),
+]
+
+
+@pytest.mark.parametrize("case", range(len(PROGRAM_CASES)))
+def test_device_programs_match_the_tree_evaluator(case):
+    """The compiled device programs, run by a numpy restatement of the device interpreter, give
+    the tree evaluator's fields: constant parts (integer arithmetic included) are folded on the
+    host, the rest is the same f64 arithmetic in the same order."""
+    d, gamma = PROGRAM_CASES[case]
+    e = expr.Expressions.from_config(d, gamma)
+    form, codes, consts = expr.compile_program(e)
+    x, y = grid()
+    t = 0.35
+    q = e.evaluate(t, x, y)
+    full = lambda v: np.broadcast_to(np.asarray(v, dtype=np.float64), x.shape)
+    rho = full(expr.run_program(codes[0], consts, dict(x=x, y=y, t=t)))
+    if form == 0:
+        rhou = full(expr.run_program(codes[1], consts, dict(x=x, y=y, t=t, rho=rho)))
+        rhov = full(expr.run_program(codes[2], consts, dict(x=x, y=y, t=t, rho=rho)))
+        en = full(expr.run_program(codes[3], consts, dict(x=x, y=y, t=t, rho=rho, rhou=rhou, rhov=rhov)))
+        got = np.stack([rho, rhou, rhov, en])
+    else:
+        u = full(expr.run_program(codes[1], consts, dict(x=x, y=y, t=t, rho=rho)))
+        v = full(expr.run_program(codes[2], consts, dict(x=x, y=y, t=t, rho=rho)))
+        p = full(expr.run_program(codes[3], consts, dict(x=x, y=y, t=t, rho=rho, u=u, v=v)))
+        got = np.stack([rho, u * rho, v * rho, p / (gamma - 1.0) + rho * (u * u + v * v) / 2.0])
+    np.testing.assert_array_equal(got, q)
+    assert all(len(c) <= expr.MAX_CODE for c in codes) and len(consts) <= expr.MAX_CONSTS
+
+
+def test_integer_parts_fold_exactly():
+    """7 / 2 is the integer 3 in the language: folded on the host, never divided in f64."""
+    e = expr.Expressions.from_config({"rho": "x + 7 / 2", "rhou": "0", "rhov": "0", "e": "1"}, 1.4)
+    _, codes, consts = expr.compile_program(e)
+    assert 3.0 in consts and 3.5 not in consts
+
+
+def test_programs_reject_what_the_device_cannot_run():
+    with pytest.raises(expr.ExprError):
+        expr.compile_program(expr.Expressions.from_config({"rho": "math::nosuch(x)", "u": "0", "v": "0", "p": "1"}, 1.4))
+    many = "; ".join(f"a{k} = x + {k}" for k in range(20)) + "; a0"
+    with pytest.raises(expr.ExprError, match="local"):
+        expr.compile_program(expr.Expressions.from_config({"rho": many, "u": "0", "v": "0", "p": "1"}, 1.4))
