@@ -68,51 +68,104 @@ def env_rank():
 
 # ------------------------------------------------------------------------------------------
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples the SM clock and the clock-event (throttle) reasons of this rank's GPU while the
+    timed region runs.  NVML is polled every 5 ms from a thread (the timed region can be well
+    under a second, shorter than nvidia-smi's sampling loop); the GPU is found by its UUID, so
+    CUDA_VISIBLE_DEVICES remapping cannot select another GPU.  Without NVML, nvidia-smi is
+    sampled instead and started before the timed region, once its first sample has arrived."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+        for cand in (uuid, "GPU-" + uuid):
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID(cand)
+            except pynvml.NVMLError:
+                continue
+        raise RuntimeError("no NVML device with this UUID")
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def poll():
+                while True:
+                    try:
+                        mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((mhz, max_mhz, ["Active" if r & b else "Not Active" for b in bits]))
+                    except nv.NVMLError:
+                        pass
+                    if self.stop_flag.wait(0.005):
+                        break
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            self.source = "nvml, 5 ms"
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
+            self.source = "nvidia-smi, 50 ms"
         except (OSError, FileNotFoundError):
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            rows = self.rows
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                rows.append((float(f[1]), float(f[2]), f[5:9]))
-            except ValueError:
-                continue
-        os.unlink(self.path)
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            rows = []
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    rows.append((float(f[1]), float(f[2]), f[5:9]))
+                except ValueError:
+                    continue
+            os.unlink(self.path)
+        else:
+            return None
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        reasons = sorted({self.NAMES[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": self.source}
 
 
 def measured_hbm_peak():

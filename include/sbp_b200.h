@@ -6,8 +6,8 @@
  * right-hand side with its SATs, and the RK4 stage update, plus the
  * euler::System / multigrid::System driver surface that calls them.  The
  * reference has no FFI of its own; each entry point below names the Rust item
- * it replaces.  A Rust -sys crate binds exactly these symbols (see
- * INTEGRATION.md).
+ * it replaces.  A Rust -sys crate binds exactly these symbols, with the same
+ * struct layouts.
  *
  * Conventions
  *  - Every function returns sbp_status (0 = SBP_OK) unless noted; on error a
@@ -70,7 +70,7 @@ typedef enum sbp_boundary_kind {
 } sbp_boundary_kind;
 
 /* sbp::operators::{Interpolation4, Interpolation8, Interpolation9, Interpolation9h2}
- * (sbp/src/operators/interpolation/*.rs).  Fine lines have 2 n - 1 points for a coarse line of
+ * (sbp/src/operators/interpolation/interpolation{4,8,9,9h2}.rs).  Fine lines have 2 n - 1 points for a coarse line of
  * n points (2 (n - 1) for Interpolation9h2). */
 typedef enum sbp_interpolation {
     SBP_INTERP4 = 0,
@@ -166,7 +166,8 @@ sbp_status sbp_metrics(int op_xi, int op_eta, const double* d_x, const double* d
  * Limits: at most 512 x 512 = 262144 points per call (larger grids return SBP_ERR_SHAPE);
  * calls share the array, so calls whose GPU work overlaps race and must not be issued; the
  * first call on each device looks the array up with cudaGetSymbolAddress and should come
- * before any stream capture.  Synchronises `stream` to read the Jacobian check. */
+ * before any stream capture; the address is kept until exit, so the entry point must not be
+ * used on a device after cudaDeviceReset.  Synchronises `stream` to read the Jacobian check. */
 sbp_status sbp_metrics_noalloc(int op_xi, int op_eta, const double* d_x, const double* d_y, int64_t ny,
                                int64_t nx, double* d_metrics, void* stream);
 

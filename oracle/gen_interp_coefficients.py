@@ -1,9 +1,9 @@
 """Generate the interpolation-operator coefficient headers from the reference's operator files.
 
-    python oracle/gen_interp_coefficients.py [reference root]
+    python oracle/gen_interp_coefficients.py <reference root>
 
-Reads sbp/src/operators/interpolation/interpolation{4,8,9,9h2}.rs of the reference (default
-/root/reference), evaluates every table entry as Rust does in both builds (each literal parsed
+Reads sbp/src/operators/interpolation/interpolation{4,8,9,9h2}.rs under the given checkout of
+the reference (a required argument), evaluates every table entry as Rust does in both builds (each literal parsed
 to the nearest f64, or f32 for the reference's f32 feature, a quotient of two literals divided
 once in that type), and writes the values, printed so that they parse back to the identical
 numbers, to
@@ -111,7 +111,9 @@ def emit(ops, prefix: str, guard: str, note: str) -> str:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python oracle/gen_interp_coefficients.py <reference root>")
+    ref = sys.argv[1]
     ops = []
     for name, fn, jf, jc, odd in OPS:
         src = open(os.path.join(ref, "sbp", "src", "operators", "interpolation", fn)).read()

@@ -42,6 +42,12 @@ UNITS = {
     "stage_f32_u4.cu": FAST32,
     "stage_f32_u9.cu": FAST32,
     "stage_f32_sbp.cu": FAST32,
+    "stage_f64_x49a.cu": EXACT,
+    "stage_f64_x49b.cu": EXACT,
+    "stage_f64_xsa.cu": EXACT,
+    "stage_f64_xsb.cu": EXACT,
+    "stage_f32_x49.cu": FAST32,
+    "stage_f32_xs.cu": FAST32,
 }
 
 

@@ -174,6 +174,9 @@ __device__ inline void eval_state(const EvalDev& E, double gamma, double t, doub
 inline const char* eval_check(const int* code, int len, int nconsts) {
     if (len < 1 || len > kEvalCode) return "program length out of range";
     int sp = 0;
+    // Programs are straight-line (EV_SELECT evaluates both operands), so a slot written in
+    // program order before every read of it is written before the read at run time.
+    bool stored[kEvalLocals] = {};
     for (int pc = 0; pc < len;) {
         const int op = code[pc++];
         const bool has_arg = op == EV_CONST || op == EV_VAR || op == EV_LOAD || op == EV_STORE || op == EV_FN1 ||
@@ -195,11 +198,13 @@ inline const char* eval_check(const int* code, int len, int nconsts) {
                 break;
             case EV_LOAD:
                 if (arg < 0 || arg >= kEvalLocals) return "local slot out of range";
+                if (!stored[arg]) return "local slot read before it is written";
                 ++sp;
                 break;
             case EV_STORE:
                 if (arg < 0 || arg >= kEvalLocals) return "local slot out of range";
                 if (sp < 1) return "stack underflow";
+                stored[arg] = true;
                 --sp;
                 break;
             case EV_NEG:

@@ -17,7 +17,8 @@
 //    without ordering between them) race on the array and must not be issued.
 //  * The first call on each device looks up the array's device address with
 //    cudaGetSymbolAddress while that device is current; make that first call before any
-//    stream capture.
+//    stream capture.  The address is kept for the life of the process, so the entry point must
+//    not be used on a device after cudaDeviceReset (which unloads the module holding the array).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -73,10 +74,11 @@ extern "C" sbp_status sbp_metrics_noalloc(int op_xi, int op_eta, const double* d
         set_error("grid %lld x %lld too small for the operators", (long long)ny, (long long)nx);
         return SBP_ERR_SHAPE;
     }
-    if (nx * ny > kNoAllocMaxPoints) {
-        set_error("grid %lld x %lld has %lld points; the fixed scratch of sbp_metrics_noalloc holds at most %lld "
+    // each side is bounded before the product is formed, so no shape can overflow it
+    if (nx > kNoAllocMaxPoints || ny > kNoAllocMaxPoints / nx) {
+        set_error("grid %lld x %lld has more than %lld points, all the fixed scratch of sbp_metrics_noalloc holds "
                   "(use sbp_metrics)",
-                  (long long)ny, (long long)nx, (long long)(nx * ny), (long long)kNoAllocMaxPoints);
+                  (long long)ny, (long long)nx, (long long)kNoAllocMaxPoints);
         return SBP_ERR_SHAPE;
     }
     double* scratch = nullptr;

@@ -12,6 +12,14 @@ const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_u4(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_u9(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty);
+// pairs of operators from two families (stage_f64_x49a/b.cu, stage_f64_xsa/b.cu, stage_f32_x49.cu,
+// stage_f32_xs.cu)
+const void* stage_ptr_f64_x49a(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f64_x49b(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f64_xsa(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f64_xsb(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f32_x49(int opx, int opy, bool upw, int ty);
+const void* stage_ptr_f32_xs(int opx, int opy, bool upw, int ty);
 // Edge (SAT) kernel entries, one per precision.
 const void* sat_ptr_f64();
 const void* sat_ptr_f32();

@@ -5,7 +5,7 @@
 
 namespace sbp {
 
-// 16-row tiles: stage_kernel; 32-row tiles: the 4-column micro-tile kernel.
+// 16-row tiles: stage_kernel; 32-row tiles: the 2 x 2 micro-tile kernel (stage_kernel_vec).
 #define CASE(OX, OY, UPW, TYV)                                                        \
     if (opx == OX && opy == OY && upw == UPW && ty == 16 && TYV == 16)                \
         return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, 16>); \

@@ -1,0 +1,28 @@
+// Instantiations of the fused stage kernel for operator pairs of two families: Upwind9-family xi operator with an Upwind4-family eta operator;
+// f64 state (reference arithmetic, built with -fmad=false).  The reference composes any (eta, xi)
+// pair of its six operators (sbp/src/operators.rs:115-150, multigrid/src/parsing.rs:153-164); the
+// upwind form needs an upwind operator in both directions, every other pair runs RHS_trad.
+#include "stage_dispatch.h"
+#include "stage_kernel.cuh"
+
+namespace sbp {
+
+#define CASE(OX, OY, UPW)                                                                           \
+    if (opx == OX && opy == OY && upw == UPW) {                                                      \
+        if (ty == 16) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 16>); \
+        if (ty == 32) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 32>); \
+    }
+
+const void* stage_ptr_f64_x49b(int opx, int opy, bool upw, int ty) {
+    CASE(UPWIND9, UPWIND4, true)
+    CASE(UPWIND9, UPWIND4, false)
+    CASE(UPWIND9, UPWIND4H2, true)
+    CASE(UPWIND9, UPWIND4H2, false)
+    CASE(UPWIND9H2, UPWIND4, true)
+    CASE(UPWIND9H2, UPWIND4, false)
+    CASE(UPWIND9H2, UPWIND4H2, true)
+    CASE(UPWIND9H2, UPWIND4H2, false)
+    return nullptr;
+}
+
+}  // namespace sbp

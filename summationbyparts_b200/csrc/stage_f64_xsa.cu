@@ -1,0 +1,29 @@
+// Instantiations of the fused stage kernel for operator pairs of two families: an upwind xi operator with an SBP4/SBP8 eta operator, and SBP4 xi with SBP8 eta;
+// f64 state (reference arithmetic, built with -fmad=false).  The reference composes any (eta, xi)
+// pair of its six operators (sbp/src/operators.rs:115-150, multigrid/src/parsing.rs:153-164); the
+// upwind form needs an upwind operator in both directions, every other pair runs RHS_trad.
+#include "stage_dispatch.h"
+#include "stage_kernel.cuh"
+
+namespace sbp {
+
+#define CASE(OX, OY, UPW)                                                                           \
+    if (opx == OX && opy == OY && upw == UPW) {                                                      \
+        if (ty == 16) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 16>); \
+        if (ty == 32) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 32>); \
+    }
+
+const void* stage_ptr_f64_xsa(int opx, int opy, bool upw, int ty) {
+    CASE(UPWIND4, SBP4, false)
+    CASE(UPWIND4, SBP8, false)
+    CASE(UPWIND4H2, SBP4, false)
+    CASE(UPWIND4H2, SBP8, false)
+    CASE(UPWIND9, SBP4, false)
+    CASE(UPWIND9, SBP8, false)
+    CASE(UPWIND9H2, SBP4, false)
+    CASE(UPWIND9H2, SBP8, false)
+    CASE(SBP4, SBP8, false)
+    return nullptr;
+}
+
+}  // namespace sbp

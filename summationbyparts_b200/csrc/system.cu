@@ -31,10 +31,14 @@ void fill_coef_table(int prec, void* out, int stride, int row);
 
 const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty) {
     using F = const void* (*)(int, int, bool, int);
-    static const F f64[] = {stage_ptr_f64_u4, stage_ptr_f64_u9, stage_ptr_f64_sbp};
-    static const F f32[] = {stage_ptr_f32_u4, stage_ptr_f32_u9, stage_ptr_f32_sbp};
-    for (F f : (prec == 0 ? f64 : f32)) {
-        const void* p = f(opx, opy, upw, ty);
+    static const F f64[] = {stage_ptr_f64_u4,   stage_ptr_f64_u9,   stage_ptr_f64_sbp, stage_ptr_f64_x49a,
+                            stage_ptr_f64_x49b, stage_ptr_f64_xsa, stage_ptr_f64_xsb};
+    static const F f32[] = {stage_ptr_f32_u4, stage_ptr_f32_u9, stage_ptr_f32_sbp, stage_ptr_f32_x49,
+                            stage_ptr_f32_xs};
+    const F* fs = prec == 0 ? f64 : f32;
+    const size_t nf = prec == 0 ? sizeof(f64) / sizeof(F) : sizeof(f32) / sizeof(F);
+    for (size_t i = 0; i < nf; ++i) {
+        const void* p = fs[i](opx, opy, upw, ty);
         if (p) return p;
     }
     return nullptr;
@@ -58,7 +62,7 @@ int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
 // Largest block: 5 planes of pad64(points) elements stay below 2^31.
 constexpr int64_t kMaxBlockPoints = (int64_t)1 << 28;
 
-// The compensated-f32 kernel of 32-row tiles is the 4-column micro-tile kernel (stage_kernel_vec).
+// The compensated-f32 kernel of 32-row tiles is the 2 x 2 micro-tile kernel (stage_kernel_vec).
 bool vec_kernel(int prec, int ty) { return prec == 1 && ty == kVecRows; }
 
 // Shared memory of one stage-kernel CTA (mirrors StageGeom in stage_kernel.cuh and VecGeom in
@@ -905,7 +909,8 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     s->staging_bytes = (size_t)s->dense_total * sizeof(double);
     e = e ?: alloc(&s->staging, s->staging_bytes);
     e = e ?: alloc((void**)&s->status, sizeof(unsigned));
-    e = e ?: alloc((void**)&s->d_sums, nblocks * sizeof(double));
+    // per-block norms, then kNormParts partial sums per block (error_terms / diff_terms)
+    e = e ?: alloc((void**)&s->d_sums, (size_t)nblocks * (1 + kNormParts) * sizeof(double));
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
@@ -1390,9 +1395,9 @@ sbp_status sbp_system_error(sbp_system* sys, double* per_instance) {
     if (!sys || !per_instance) return SBP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(sys->device);
     cudaStream_t st = sys->st();
-    SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sys->nblocks * sizeof(double), st));
     SBP_TRY_CUDA(error_terms(sys->d_blocks, sys->d_inst, sys->nblocks, sys->gamma, sys->xy, sys->prec, sys->prev_hi,
-                             sys->prev_lo, sys->hw, sys->d_hoff, sys->max_points, sys->d_sums, st));
+                             sys->prev_lo, sys->hw, sys->d_hoff, sys->max_points, sys->d_sums,
+                             sys->d_sums + sys->nblocks, st));
     std::vector<double> sums(sys->nblocks);
     SBP_TRY_CUDA(cudaMemcpyAsync(sums.data(), sys->d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
@@ -1409,10 +1414,10 @@ sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double
     const BlockDev& B = sys->hb[block];
     const int64_t n = (int64_t)B.nx * B.ny;
     SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
-    SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sizeof(double), st));
     const double* hx = sys->hw + sys->hoff[block];
     SBP_TRY_CUDA(diff_terms(sys->d_blocks + block, sys->prec, sys->prev_hi, sys->prev_lo,
-                            static_cast<const double*>(sys->staging), hx, hx + B.nx, n, sys->d_sums, st));
+                            static_cast<const double*>(sys->staging), hx, hx + B.nx, n, sys->d_sums,
+                            sys->d_sums + 1, st));
     double s = 0;
     SBP_TRY_CUDA(cudaMemcpyAsync(&s, sys->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
@@ -1446,11 +1451,19 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads) 
     std::fill(sys->active.begin(), sys->active.end(), 1);
     static const int cand[][3] = {{16, kTileX, kStageThreads}, {32, kTileX, kStageThreads}};
     const size_t ts = sys->tsize();
-    // save state and times
-    void* save_hi = nullptr;
-    void* save_lo = nullptr;
-    SBP_TRY_CUDA(cudaMalloc(&save_hi, sys->nq * ts));
-    if (sys->prev_lo) SBP_TRY_CUDA(cudaMalloc(&save_lo, sys->nq * ts));
+    // save state and times; the copies are freed on every return path
+    struct Saved {
+        void* hi = nullptr;
+        void* lo = nullptr;
+        ~Saved() {
+            if (hi) cudaFree(hi);
+            if (lo) cudaFree(lo);
+        }
+    } saved;
+    SBP_TRY_CUDA(cudaMalloc(&saved.hi, sys->nq * ts));
+    if (sys->prev_lo) SBP_TRY_CUDA(cudaMalloc(&saved.lo, sys->nq * ts));
+    void* const save_hi = saved.hi;
+    void* const save_lo = saved.lo;
     cudaStream_t st = sys->st();
     SBP_TRY(sync_times(sys));
     std::vector<InstanceDev> save_inst = sys->hi;
@@ -1488,8 +1501,6 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads) 
     upload_instances(sys);
     cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st);
     cudaStreamSynchronize(st);
-    cudaFree(save_hi);
-    if (save_lo) cudaFree(save_lo);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     clear_error();
@@ -1589,9 +1600,8 @@ sbp_status sbp_system_advance_adaptive(sbp_system* sys, double dt, double* guess
         SBP_TRY(integrate_tableau(sys, T, guess, fut, fut2));
         time += guess;
         SBP_TRY_CUDA(pack_state(sys->d_blocks, 1, sys->d_poff4, 0, 0, fut2, nullptr, sys->staging, sys->max_points, st));
-        SBP_TRY_CUDA(cudaMemsetAsync(sys->d_sums, 0, sizeof(double), st));
         SBP_TRY_CUDA(diff_terms(sys->d_blocks, 0, sys->prev_hi, nullptr, static_cast<const double*>(sys->staging), hx,
-                                hx + B.nx, n, sys->d_sums, st));
+                                hx + B.nx, n, sys->d_sums, sys->d_sums + 1, st));
         double e2 = 0.0;
         SBP_TRY_CUDA(cudaMemcpyAsync(&e2, sys->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));
         SBP_TRY_CUDA(cudaStreamSynchronize(st));

@@ -67,7 +67,7 @@ __device__ __forceinline__ double state_at(int prec, const void* q_hi, const voi
 __global__ void error_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst, double gamma,
                              const double* __restrict__ xy, int prec, const void* q_hi, const void* q_lo,
                              const double* __restrict__ hw, const int64_t* __restrict__ h_off,
-                             double* __restrict__ sums) {
+                             double* __restrict__ partials) {
     const int b = blockIdx.y;
     const BlockDev& B = blocks[b];
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
@@ -92,13 +92,13 @@ __global__ void error_kernel(const BlockDev* __restrict__ blocks, const Instance
     if (threadIdx.x < 32) {
         s = threadIdx.x < (kT / 32) ? red[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) atomicAdd(sums + b, s);
+        if (threadIdx.x == 0) partials[(int64_t)b * gridDim.x + blockIdx.x] = s;
     }
 }
 
 __global__ void diff_kernel(const BlockDev* __restrict__ blk, int prec, const void* q_hi, const void* q_lo,
                             const double* __restrict__ dense, const double* __restrict__ hx,
-                            const double* __restrict__ hy, double* __restrict__ sum) {
+                            const double* __restrict__ hy, double* __restrict__ partials) {
     const BlockDev& B = *blk;
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     double s = 0.0;
@@ -116,8 +116,18 @@ __global__ void diff_kernel(const BlockDev* __restrict__ blk, int prec, const vo
     if (threadIdx.x < 32) {
         s = threadIdx.x < (kT / 32) ? red[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) atomicAdd(sum, s);
+        if (threadIdx.x == 0) partials[blockIdx.x] = s;
     }
+}
+
+// out[j] = sum of partials[j * nper .. j * nper + nper) in index order: the norms come out the
+// same on every run (no floating-point atomics).
+__global__ void sum_partials_kernel(const double* __restrict__ partials, int nper, int nsum, double* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nsum) return;
+    double s = 0.0;
+    for (int k = 0; k < nper; ++k) s += partials[(int64_t)j * nper + k];
+    out[j] = s;
 }
 
 __global__ void max_speed_kernel(const BlockDev* __restrict__ blocks, int prec, const void* q_hi,
@@ -243,6 +253,13 @@ dim3 per_block_grid(int nblocks, int64_t max_points) {
     return dim3((unsigned)gx, (unsigned)nblocks, 1);
 }
 
+// Grid of the norm kernels: at most kNormParts CTAs per block, each writing one partial sum.
+dim3 norm_grid(int nblocks, int64_t max_points) {
+    dim3 g = per_block_grid(nblocks, max_points);
+    if (g.x > (unsigned)kNormParts) g.x = kNormParts;
+    return g;
+}
+
 int flat_grid(int64_t n) {
     int64_t g = (n + kT - 1) / kT;
     if (g > 148 * 32) g = 148 * 32;
@@ -272,15 +289,20 @@ cudaError_t vortex_init(const BlockDev* blocks, const InstanceDev* inst, int nbl
 
 cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nblocks, double gamma,
                         const double* xy, int prec, const void* q_hi, const void* q_lo, const double* hweights,
-                        const int64_t* h_off, int64_t max_points, double* block_sums, cudaStream_t st) {
-    error_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, gamma, xy, prec, q_hi, q_lo,
-                                                                    hweights, h_off, block_sums);
+                        const int64_t* h_off, int64_t max_points, double* block_sums, double* partials,
+                        cudaStream_t st) {
+    const dim3 g = norm_grid(nblocks, max_points);
+    error_kernel<<<g, kT, 0, st>>>(blocks, inst, gamma, xy, prec, q_hi, q_lo, hweights, h_off, partials);
+    sum_partials_kernel<<<(nblocks + kT - 1) / kT, kT, 0, st>>>(partials, (int)g.x, nblocks, block_sums);
     return cudaGetLastError();
 }
 
 cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
-                       const double* hx, const double* hy, int64_t max_points, double* sum, cudaStream_t st) {
-    diff_kernel<<<per_block_grid(1, max_points).x, kT, 0, st>>>(block, prec, q_hi, q_lo, dense, hx, hy, sum);
+                       const double* hx, const double* hy, int64_t max_points, double* sum, double* partials,
+                       cudaStream_t st) {
+    const dim3 g = norm_grid(1, max_points);
+    diff_kernel<<<g.x, kT, 0, st>>>(block, prec, q_hi, q_lo, dense, hx, hy, partials);
+    sum_partials_kernel<<<1, 32, 0, st>>>(partials, (int)g.x, 1, sum);
     return cudaGetLastError();
 }
 

@@ -23,15 +23,23 @@ cudaError_t vortex_init(const BlockDev* blocks, const InstanceDev* inst, int nbl
                         double t, const double* xy, int prec, void* q_hi, void* q_lo, int64_t max_points,
                         cudaStream_t st);
 
-// Field::h2_err terms against the vortex at each block's instance time: block_sums[b] += sum of
-// (q - vortex)^2 hx hy over the block (euler/src/lib.rs:377-431).
+// Partial sums per block of the norm kernels below (the `partials` buffers hold
+// kNormParts * nblocks doubles).
+constexpr int kNormParts = 128;
+
+// Field::h2_err terms against the vortex at each block's instance time: block_sums[b] = sum of
+// (q - vortex)^2 hx hy over the block (euler/src/lib.rs:377-431).  Each CTA writes a partial
+// sum and the partials are added in a fixed order, so the result is the same on every run.
 cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nblocks, double gamma,
                         const double* xy, int prec, const void* q_hi, const void* q_lo, const double* hweights,
-                        const int64_t* h_off, int64_t max_points, double* block_sums, cudaStream_t st);
+                        const int64_t* h_off, int64_t max_points, double* block_sums, double* partials,
+                        cudaStream_t st);
 
-// Field::h2_err of one block's state against a dense (4, ny, nx) f64 field: *sum += terms.
+// Field::h2_err of one block's state against a dense (4, ny, nx) f64 field: *sum = terms
+// (partials: kNormParts doubles).
 cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
-                       const double* hx, const double* hy, int64_t max_points, double* sum, cudaStream_t st);
+                       const double* hx, const double* hy, int64_t max_points, double* sum, double* partials,
+                       cudaStream_t st);
 
 // max |uhat|, max |vhat| per block (multigrid/src/system.rs:555-580), as ordered bit patterns.
 cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,

@@ -77,6 +77,13 @@ def test_programs_are_validated_and_required():
     consts = np.array([1.0])
     st = _capi.lib.sbp_system_set_eval(g.h, 0, ptrs, lens, consts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1)
     assert st == 1 and b"underflow" in _capi.lib.sbp_last_error()
+    # program 0 reads local slot 2 (EV_LOAD = 3) that nothing has written
+    unread = [[3, 2], [1, 0], [1, 0], [1, 0]]
+    arrs = [np.array(c, dtype=np.int32) for c in unread]
+    ptrs = (ctypes.POINTER(ctypes.c_int32) * 4)(*[a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) for a in arrs])
+    lens = (ctypes.c_int32 * 4)(*[len(c) for c in unread])
+    st = _capi.lib.sbp_system_set_eval(g.h, 0, ptrs, lens, consts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1)
+    assert st == 1 and b"read before it is written" in _capi.lib.sbp_last_error()
     g.close()
 
 

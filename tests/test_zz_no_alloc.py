@@ -45,3 +45,6 @@ def test_noalloc_refuses_grids_beyond_its_scratch():
     st = _capi.lib.sbp_metrics_noalloc(0, 0, p, p, 513, 513, p, None)
     assert st == 2  # SBP_ERR_SHAPE
     assert "262144" in _capi.lib.sbp_last_error().decode()
+    # sides whose product would overflow 64 bits are refused too, not wrapped to a small size
+    for ny, nx in ((1 << 33, 1 << 31), (1 << 31, 1 << 33), (2, 1 << 62)):
+        assert _capi.lib.sbp_metrics_noalloc(0, 0, p, p, ny, nx, p, None) == 2, (ny, nx)
