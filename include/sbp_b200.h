@@ -54,8 +54,11 @@ typedef enum sbp_operator {
 typedef enum sbp_dtype { SBP_F64 = 0, SBP_F32 = 1 } sbp_dtype;
 
 /* SBP_PRECISION_F64: the reference's f64 arithmetic, operation for operation.
- * SBP_PRECISION_F32_COMPENSATED: stencils, fluxes and dissipation in f32, the RK4 state kept as
- * a compensated (hi, lo) f32 pair; metrics built in f64, SAT terms and norms in f64. */
+ * SBP_PRECISION_F32_COMPENSATED: stencils, fluxes and dissipation in f32 on deviations from each
+ * instance's free stream (so f32 rounding is relative to the deviation, not to the state), the
+ * RK4 state kept as that deviation in a compensated (hi, lo) f32 pair; metrics built in f64,
+ * the free-stream dissipation term, SAT terms and norms in f64.  Every state entry point below
+ * takes and returns the absolute state. */
 typedef enum sbp_precision { SBP_PRECISION_F64 = 0, SBP_PRECISION_F32_COMPENSATED = 1 } sbp_precision;
 
 /* euler::BoundaryCharacteristic (euler/src/lib.rs:737-745): This, Grid(neighbour), Vortex,
@@ -186,7 +189,9 @@ sbp_status sbp_system_destroy(sbp_system* sys);
 sbp_status sbp_system_set_force_trad(sbp_system* sys, int force_trad);
 
 /* Vortex parameters of one instance (or all when instance < 0); used by vortex initial data,
- * SBP_BC_VORTEX boundaries and sbp_system_error. */
+ * SBP_BC_VORTEX boundaries and sbp_system_error.  Their free stream is the instance's reference
+ * state in the compensated precision; a compensated system's state is re-expressed against the
+ * new reference, so the state itself is unchanged. */
 sbp_status sbp_system_set_vortex(sbp_system* sys, int instance, const sbp_vortex_params* vp);
 /* Field::vortex / SingleThreadedSystem::vortex (euler/src/lib.rs:319-328, system.rs:477-481):
  * state of every block of the instance(s) := the vortex at time t.  instance < 0 = all. */
@@ -264,7 +269,9 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads);
 
 /* Stream the system launches on (cudaStream_t as void*; NULL = a stream owned by the system). */
 sbp_status sbp_system_set_stream(sbp_system* sys, void* stream);
-/* Device pointer to one block's current state plane set (f64 or f32 hi), for zero-copy use. */
+/* Device pointer to one block's current state plane set, for zero-copy use: the state in an f64
+ * system; in a compensated system the f32 hi planes of the state's deviation from the
+ * instance's free stream (sbp_system_get_state_all_device gives the state itself). */
 sbp_status sbp_system_device_state(sbp_system* sys, int block, void** d_q);
 /* Explicit Runge-Kutta tableaus of utils/integrate/src/lib.rs:30-152. */
 typedef enum sbp_tableau {

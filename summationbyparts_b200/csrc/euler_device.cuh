@@ -29,6 +29,7 @@ struct BlockDev {
     int bc_aux2[4];  // BC_MULTIGRID: number of segments
     int64_t q_off, m_off, x_off;
     int64_t e_off;  // slot of this block's first edge point in the edge-k buffer (see edge_index)
+    int64_t r_off;  // compensated f32: this block's free-stream dissipation plane (see InstanceDev)
     double idx_xi, idx_eta;  // 1/(1/(n-1)) per direction, f64
     float idx_xi_f, idx_eta_f;
     double hi_xi, hi_eta;  // SAT penalty (n-1)/H_0 (euler/src/lib.rs:1033-1037)
@@ -44,6 +45,14 @@ __host__ __device__ __forceinline__ int edge_index(int row, int col, int nx, int
 }
 __host__ __device__ constexpr int64_t edge_count(int64_t nx, int64_t ny) { return 2 * nx + 2 * ny - 4; }
 
+// Reference state of the compensated-f32 form, as f32 constants of the deviation arithmetic:
+// the conserved state q_r = (rho_r, m_r, n_r, e_r), velocity (u_r, v_r), pressure p_r,
+// total enthalpy H_r = e_r + p_r, sound speed c_r and c_r^2, gamma / rho_r.
+struct RefState {
+    float q[4];
+    float u, v, p, h, c, c2, g_rho;
+};
+
 struct InstanceDev {
     double dt, time;
     double ca[3];  // A-tableau entries times dt for stages 2..4 (0.5dt, 0.5dt, 1.0dt)
@@ -51,6 +60,11 @@ struct InstanceDev {
     int nvort;
     double x0[5], y0[5], rstar[5], eps[5];
     double mach;
+    // Compensated-f32 systems store the state of every block of the instance as its deviation
+    // from qref, the free stream of the instance's vortex parameters (rho 1, u 1, v 0,
+    // p 1/(gamma M^2)); f64 systems store the state itself.
+    double qref[4];
+    RefState ref;
 };
 
 // pressure (euler/src/lib.rs:478-480)

@@ -250,9 +250,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll
             for (int b = 0; b < P1B; ++b)
                 if (pt[b] >= 0)
-                    pointwise<float, UPW, false>(qv[b], m[b], gamma, sE + (oxi[b] >= 0 ? oxi[b] : 0), XA,
-                                                 sF + (oeta[b] >= 0 ? oeta[b] : 0), YA, oxi[b] >= 0, oeta[b] >= 0,
-                                                 bad);
+                    pointwise_dev<UPW>(qv[b], m[b], gamma, I.ref, sE + (oxi[b] >= 0 ? oxi[b] : 0), XA,
+                                       sF + (oeta[b] >= 0 ? oeta[b] : 0), YA, oxi[b] >= 0, oeta[b] >= 0, bad);
         }
 
         // Phase-2 operands of this thread (detJ and component 0's RK operands), loaded before
@@ -267,13 +266,15 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const float* srcb[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) srcb[a] = a < nsrc ? src[a] + qoff : nullptr;
-        float detj[2][2], opn[3][2][2];
+        float detj[2][2], rinf[2][2], opn[3][2][2];
+        const float* rb = UPW ? A.rinf + B.r_off : nullptr;
 #pragma unroll
         for (int u = 0; u < 2; ++u)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const bool ok = rok[u] && cok[j];
                 detj[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
+                rinf[u][j] = (UPW && ok) ? __ldg(rb + (e0 + off[u][j])) : 0.0f;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
             }
@@ -321,6 +322,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll 1
             for (int cc = 0; cc < 4; ++cc) {
                 const int ce = e0 + cc * np;
+                const float qr = I.ref.q[cc];  // reference state (free-stream dissipation term)
                 float nxt[3][2][2];
                 if (cc < 3) {
 #pragma unroll
@@ -363,7 +365,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         const float exv = u == 0 ? ex[j].x : ex[j].y, dxv = u == 0 ? dx[j].x : dx[j].y;
                         const float eyv = j == 0 ? ey[u].x : ey[u].y, ayv = j == 0 ? ay[u].x : ay[u].y;
                         float kc;
-                        if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) / detj[u][j];
+                        if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) / detj[u][j] + qr * rinf[u][j];
                         else kc = (-exv - eyv) / detj[u][j];
                         const int e = ce + off[u][j];
                         if (edge[u][j]) {

@@ -135,6 +135,7 @@ struct sbp_system {
     void *prev_hi = nullptr, *prev_lo = nullptr, *acc_hi = nullptr, *acc_lo = nullptr, *uA = nullptr, *uB = nullptr;
     double* met64 = nullptr;
     float* met32 = nullptr;
+    float* rinf = nullptr;  // compensated f32: free-stream dissipation planes (BlockDev::r_off)
     double* xy = nullptr;
     double* hw = nullptr;
     int64_t* d_hoff = nullptr;
@@ -216,7 +217,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -224,6 +225,24 @@ void destroy_all(sbp_system* s) {
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+}
+
+// Free-stream dissipation planes of the compensated form for the upwind blocks of one instance
+// (instance < 0: all), from the instances' reference states on the device.
+sbp_status build_free_stream_dissipation(sbp_system* s, int instance) {
+    if (!s->rinf) return SBP_OK;
+    cudaStream_t st = s->st();
+    for (int b = 0; b < s->nblocks; ++b) {
+        const BlockDev& B = s->hb[b];
+        if (instance >= 0 && B.instance != instance) continue;
+        OpInfo ox, oy;
+        op_info(B.op_xi, ox);
+        op_info(B.op_eta, oy);
+        if (!(ox.upwind && oy.upwind)) continue;
+        SBP_TRY_CUDA(free_stream_dissipation(s->d_blocks + b, s->d_inst, s->gamma, B.op_xi, B.op_eta, B.nx, B.ny,
+                                             s->met64, static_cast<double*>(s->staging), s->rinf, st));
+    }
+    return SBP_OK;
 }
 
 sbp_status upload_instances(sbp_system* s) {
@@ -255,6 +274,27 @@ void set_dt_host(InstanceDev& I, double dt) {
     I.cb[3] = (1.0 / 6.0) * dt;
 }
 
+// Reference state of an instance: the free stream of its vortex parameters (rho 1, u 1, v 0,
+// p = 1 / (gamma M^2); euler/src/vortex.rs:26-40), against which compensated systems store the
+// state, and its f32 constants for the stage kernels.
+void set_reference(InstanceDev& I, double gamma) {
+    const double p = 1.0 / (gamma * I.mach * I.mach);
+    const double rho = 1.0, u = 1.0, v = 0.0;
+    I.qref[0] = rho;
+    I.qref[1] = rho * u;
+    I.qref[2] = rho * v;
+    I.qref[3] = p / (gamma - 1.0) + rho * (u * u + v * v) / 2.0;
+    RefState& R = I.ref;
+    for (int c = 0; c < 4; ++c) R.q[c] = float(I.qref[c]);
+    R.u = float(u);
+    R.v = float(v);
+    R.p = float(p);
+    R.h = float(I.qref[3] + p);
+    R.c2 = float(gamma * p / rho);
+    R.c = float(std::sqrt(gamma * p / rho));
+    R.g_rho = float(gamma / rho);
+}
+
 template <class T>
 StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     StageArgs<T> a{};
@@ -277,6 +317,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.new_lo = static_cast<T*>(s->prev_lo);
     a.met = s->prec == 0 ? reinterpret_cast<const T*>(s->met64) : reinterpret_cast<const T*>(s->met32);
     a.met64 = s->met64;
+    a.rinf = s->rinf;
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
     a.kedge = static_cast<T*>(s->kedge);
@@ -856,6 +897,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
             }
         }
         B.q_off = s->nq;
+        B.r_off = s->nq / 4;
         B.m_off = s->nm;
         B.x_off = s->nx2;
         B.e_off = s->nedge;
@@ -882,6 +924,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         set_dt_host(I, NAN);
         I.time = 0.0;
         I.mach = 0.5;
+        set_reference(I, gamma);
     }
     s->active.assign(ninstances, 1);
     // allocations
@@ -898,6 +941,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     if (precision == SBP_PRECISION_F32_COMPENSATED) {
         e = e ?: alloc(&s->prev_lo, s->nq * ts);
         e = e ?: alloc((void**)&s->met32, s->nm * sizeof(float));
+        e = e ?: alloc((void**)&s->rinf, (s->nq / 4) * sizeof(float));
     }
     e = e ?: alloc((void**)&s->met64, s->nm * sizeof(double));
     e = e ?: alloc((void**)&s->xy, s->nx2 * sizeof(double));
@@ -986,6 +1030,15 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     }
     if (e == cudaSuccess && s->met32) e = narrow_f32(s->met64, s->met32, s->nm, st);
     if (e != cudaSuccess) return fail(cuda_status(e, "metrics"));
+    if (s->rinf) {
+        // the state starts at zero: in the compensated form a deviation of -qref
+        e = cudaMemsetAsync(s->staging, 0, s->staging_bytes, st);
+        e = e ?: unpack_state(s->d_blocks, s->d_inst, nblocks, s->d_poff4, s->prec, SBP_F64, s->staging, s->prev_hi,
+                              s->prev_lo, s->max_points, st);
+        if (e != cudaSuccess) return fail(cuda_status(e, "initial state"));
+        const sbp_status rs = build_free_stream_dissipation(s, -1);
+        if (rs != SBP_OK) return fail(rs);
+    }
     sbp_status cs = check_status(s);
     if (cs != SBP_OK) {
         set_error("non-positive Jacobian determinant in the grid (Metrics::new asserts detj > 0)");
@@ -1030,6 +1083,13 @@ sbp_status sbp_system_set_vortex(sbp_system* sys, int instance, const sbp_vortex
     }
     cudaSetDevice(sys->device);
     SBP_TRY(sync_times(sys));
+    cudaStream_t st = sys->st();
+    // A compensated system keeps each instance's state as a deviation from the instance's
+    // reference state, which follows the vortex's free stream: the state is taken out as the
+    // absolute state and stored again against the new reference.
+    if (sys->prec == 1)
+        SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->d_inst, sys->nblocks, sys->d_poff4, sys->prec, SBP_F64,
+                                sys->prev_hi, sys->prev_lo, sys->staging, sys->max_points, st));
     for (int i = 0; i < sys->ninst; ++i) {
         if (instance >= 0 && i != instance) continue;
         InstanceDev& I = sys->hi[i];
@@ -1041,8 +1101,16 @@ sbp_status sbp_system_set_vortex(sbp_system* sys, int instance, const sbp_vortex
             I.eps[k] = vp->eps[k];
         }
         I.mach = vp->mach;
+        set_reference(I, sys->gamma);
     }
-    return upload_instances(sys);
+    SBP_TRY(upload_instances(sys));
+    if (sys->prec == 1) {
+        SBP_TRY_CUDA(unpack_state(sys->d_blocks, sys->d_inst, sys->nblocks, sys->d_poff4, sys->prec, SBP_F64,
+                                  sys->staging, sys->prev_hi, sys->prev_lo, sys->max_points, st));
+        SBP_TRY(build_free_stream_dissipation(sys, instance));
+        SBP_TRY_CUDA(cudaStreamSynchronize(st));
+    }
+    return SBP_OK;
 }
 
 sbp_status sbp_system_init_vortex(sbp_system* sys, int instance, double t) {
@@ -1068,7 +1136,7 @@ sbp_status sbp_system_set_state(sbp_system* sys, int block, const double* q) {
                                        n * sizeof(double), n * sizeof(double), 4, cudaMemcpyHostToDevice, st));
     } else {
         SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
-        SBP_TRY_CUDA(unpack_state(sys->d_blocks + block, 1, sys->d_zero, sys->prec, 0, sys->staging, sys->prev_hi,
+        SBP_TRY_CUDA(unpack_state(sys->d_blocks + block, sys->d_inst, 1, sys->d_zero, sys->prec, 0, sys->staging, sys->prev_hi,
                                   sys->prev_lo, n, st));
     }
     SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
@@ -1087,7 +1155,7 @@ sbp_status sbp_system_get_state(sbp_system* sys, int block, double* q) {
         SBP_TRY_CUDA(cudaMemcpy2DAsync(q, n * sizeof(double), static_cast<double*>(sys->prev_hi) + B.q_off,
                                        B.npad * sizeof(double), n * sizeof(double), 4, cudaMemcpyDeviceToHost, st));
     } else {
-        SBP_TRY_CUDA(pack_state(sys->d_blocks + block, 1, sys->d_zero, sys->prec, 0, sys->prev_hi, sys->prev_lo,
+        SBP_TRY_CUDA(pack_state(sys->d_blocks + block, sys->d_inst, 1, sys->d_zero, sys->prec, 0, sys->prev_hi, sys->prev_lo,
                                 sys->staging, n, st));
         SBP_TRY_CUDA(cudaMemcpyAsync(q, sys->staging, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
@@ -1107,7 +1175,7 @@ sbp_status sbp_system_set_state_all(sbp_system* sys, int dtype, const void* q) {
     cudaStream_t st = sys->st();
     const size_t bytes = (size_t)sys->dense_total * (dtype == SBP_F64 ? 8 : 8);
     SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, bytes, cudaMemcpyHostToDevice, st));
-    SBP_TRY_CUDA(unpack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+    SBP_TRY_CUDA(unpack_state(sys->d_blocks, sys->d_inst, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
                               dtype, sys->staging, sys->prev_hi, sys->prev_lo, sys->max_points, st));
     SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
@@ -1120,7 +1188,7 @@ sbp_status sbp_system_get_state_all(sbp_system* sys, int dtype, void* q) {
     cudaSetDevice(sys->device);
     cudaStream_t st = sys->st();
     const size_t bytes = (size_t)sys->dense_total * 8;
-    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->d_inst, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
                             dtype, sys->prev_hi, sys->prev_lo, sys->staging, sys->max_points, st));
     SBP_TRY_CUDA(cudaMemcpyAsync(q, sys->staging, bytes, cudaMemcpyDeviceToHost, st));
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
@@ -1132,7 +1200,7 @@ sbp_status sbp_system_get_state_all_device(sbp_system* sys, int dtype, void* d_q
     if (!sys || !d_q || (dtype != SBP_F64 && dtype != SBP_F32)) return SBP_ERR_INVALID_ARGUMENT;
     cudaSetDevice(sys->device);
     cudaStream_t st = sys->st();
-    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
+    SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->d_inst, sys->nblocks, dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8, sys->prec,
                             dtype, sys->prev_hi, sys->prev_lo, d_q, sys->max_points, st));
     SBP_TRY_CUDA(cudaStreamSynchronize(st));
     return SBP_OK;
@@ -1256,10 +1324,10 @@ sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in,
         const int64_t o1 = c.b1 < sys->nblocks ? 8 * sys->dense_off[c.b1] : 8 * sys->dense_total;
         SBP_TRY_CUDA(cudaStreamWaitEvent(c.st, sys->ev_fork, 0));
         SBP_TRY_CUDA(cudaMemcpyAsync(stg + o0, in + o0, o1 - o0, cudaMemcpyHostToDevice, c.st));
-        SBP_TRY_CUDA(unpack_state(sys->d_blocks + c.b0, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->staging,
+        SBP_TRY_CUDA(unpack_state(sys->d_blocks + c.b0, sys->d_inst, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->staging,
                                   sys->prev_hi, sys->prev_lo, sys->max_points, c.st));
         for (int64_t k = 0; k < nsteps; ++k) SBP_TRY_CUDA(cudaGraphLaunch(c.gexec, c.st));
-        SBP_TRY_CUDA(pack_state(sys->d_blocks + c.b0, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->prev_hi,
+        SBP_TRY_CUDA(pack_state(sys->d_blocks + c.b0, sys->d_inst, c.b1 - c.b0, poff + c.b0, sys->prec, dtype, sys->prev_hi,
                                 sys->prev_lo, sys->staging, sys->max_points, c.st));
         SBP_TRY_CUDA(cudaMemcpyAsync(out + o0, stg + o0, o1 - o0, cudaMemcpyDeviceToHost, c.st));
         SBP_TRY_CUDA(cudaEventRecord(c.done, c.st));
@@ -1309,7 +1377,7 @@ sbp_status sbp_system_max_dt(sbp_system* sys, int instance, double* dt) {
     cudaSetDevice(sys->device);
     cudaStream_t st = sys->st();
     SBP_TRY_CUDA(cudaMemsetAsync(sys->d_speeds, 0, 2 * sys->nblocks * sizeof(unsigned long long), st));
-    SBP_TRY_CUDA(max_speeds(sys->d_blocks, sys->nblocks, sys->prec, sys->prev_hi, sys->met64, sys->max_points,
+    SBP_TRY_CUDA(max_speeds(sys->d_blocks, sys->d_inst, sys->nblocks, sys->prec, sys->prev_hi, sys->prev_lo, sys->met64, sys->max_points,
                             sys->d_speeds, st));
     std::vector<unsigned long long> sp(2 * sys->nblocks);
     SBP_TRY_CUDA(cudaMemcpyAsync(sp.data(), sys->d_speeds, sp.size() * sizeof(unsigned long long),
@@ -1415,7 +1483,7 @@ sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double
     const int64_t n = (int64_t)B.nx * B.ny;
     SBP_TRY_CUDA(cudaMemcpyAsync(sys->staging, q, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
     const double* hx = sys->hw + sys->hoff[block];
-    SBP_TRY_CUDA(diff_terms(sys->d_blocks + block, sys->prec, sys->prev_hi, sys->prev_lo,
+    SBP_TRY_CUDA(diff_terms(sys->d_blocks + block, sys->d_inst, sys->prec, sys->prev_hi, sys->prev_lo,
                             static_cast<const double*>(sys->staging), hx, hx + B.nx, n, sys->d_sums,
                             sys->d_sums + 1, st));
     double s = 0;
@@ -1599,8 +1667,8 @@ sbp_status sbp_system_advance_adaptive(sbp_system* sys, double dt, double* guess
         }
         SBP_TRY(integrate_tableau(sys, T, guess, fut, fut2));
         time += guess;
-        SBP_TRY_CUDA(pack_state(sys->d_blocks, 1, sys->d_poff4, 0, 0, fut2, nullptr, sys->staging, sys->max_points, st));
-        SBP_TRY_CUDA(diff_terms(sys->d_blocks, 0, sys->prev_hi, nullptr, static_cast<const double*>(sys->staging), hx,
+        SBP_TRY_CUDA(pack_state(sys->d_blocks, sys->d_inst, 1, sys->d_poff4, 0, 0, fut2, nullptr, sys->staging, sys->max_points, st));
+        SBP_TRY_CUDA(diff_terms(sys->d_blocks, sys->d_inst, 0, sys->prev_hi, nullptr, static_cast<const double*>(sys->staging), hx,
                                 hx + B.nx, n, sys->d_sums, sys->d_sums + 1, st));
         double e2 = 0.0;
         SBP_TRY_CUDA(cudaMemcpyAsync(&e2, sys->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));

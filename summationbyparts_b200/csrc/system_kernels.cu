@@ -2,6 +2,7 @@
 // state packing.  Compiled with -fmad=false so the f64 arithmetic matches the reference's.
 #include <cuda_runtime.h>
 
+#include "op_apply.h"
 #include "system_kernels.h"
 
 namespace sbp {
@@ -35,6 +36,19 @@ __device__ __forceinline__ void split_f32(double v, float& hi, float& lo) {
     lo = float(v - double(hi));
 }
 
+// Store the absolute f64 state value v at element g: as is in f64, as the (hi, lo) split of its
+// deviation from the instance's reference state in the compensated form.
+__device__ __forceinline__ void store_state(int prec, void* q_hi, void* q_lo, int64_t g, double v, double qref) {
+    if (prec == 0) {
+        static_cast<double*>(q_hi)[g] = v;
+    } else {
+        float h, l;
+        split_f32(v - qref, h, l);
+        static_cast<float*>(q_hi)[g] = h;
+        static_cast<float*>(q_lo)[g] = l;
+    }
+}
+
 __global__ void vortex_init_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst,
                                    int instance, double gamma, double t, const double* __restrict__ xy, int prec,
                                    void* q_hi, void* q_lo) {
@@ -45,23 +59,15 @@ __global__ void vortex_init_kernel(const BlockDev* __restrict__ blocks, const In
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double q[4];
         vortex_point(I, gamma, t, xy[B.x_off + i], xy[B.x_off + np + i], q);
-        for (int c = 0; c < 4; ++c) {
-            const int64_t g = B.q_off + c * np + i;
-            if (prec == 0) {
-                static_cast<double*>(q_hi)[g] = q[c];
-            } else {
-                float h, l;
-                split_f32(q[c], h, l);
-                static_cast<float*>(q_hi)[g] = h;
-                static_cast<float*>(q_lo)[g] = l;
-            }
-        }
+        for (int c = 0; c < 4; ++c) store_state(prec, q_hi, q_lo, B.q_off + c * np + i, q[c], I.qref[c]);
     }
 }
 
-__device__ __forceinline__ double state_at(int prec, const void* q_hi, const void* q_lo, int64_t g) {
+// Absolute state at element g (qref: the instance's reference value of the component, added to
+// the stored deviation in the compensated form; hi + lo is exact in f64).
+__device__ __forceinline__ double state_at(int prec, const void* q_hi, const void* q_lo, int64_t g, double qref) {
     if (prec == 0) return static_cast<const double*>(q_hi)[g];
-    return double(static_cast<const float*>(q_hi)[g]) + double(static_cast<const float*>(q_lo)[g]);
+    return qref + (double(static_cast<const float*>(q_hi)[g]) + double(static_cast<const float*>(q_lo)[g]));
 }
 
 __global__ void error_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst, double gamma,
@@ -80,7 +86,7 @@ __global__ void error_kernel(const BlockDev* __restrict__ blocks, const Instance
         double v[4];
         vortex_point(I, gamma, I.time, xy[B.x_off + i], xy[B.x_off + np + i], v);
         for (int c = 0; c < 4; ++c) {
-            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i) - v[c];
+            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i, I.qref[c]) - v[c];
             s += d * d * hx[col] * hy[row];
         }
     }
@@ -96,16 +102,18 @@ __global__ void error_kernel(const BlockDev* __restrict__ blocks, const Instance
     }
 }
 
-__global__ void diff_kernel(const BlockDev* __restrict__ blk, int prec, const void* q_hi, const void* q_lo,
-                            const double* __restrict__ dense, const double* __restrict__ hx,
-                            const double* __restrict__ hy, double* __restrict__ partials) {
+__global__ void diff_kernel(const BlockDev* __restrict__ blk, const InstanceDev* __restrict__ inst, int prec,
+                            const void* q_hi, const void* q_lo, const double* __restrict__ dense,
+                            const double* __restrict__ hx, const double* __restrict__ hy,
+                            double* __restrict__ partials) {
     const BlockDev& B = *blk;
+    const InstanceDev& I = inst[B.instance];
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int row = (int)(i / B.nx), col = (int)(i - (int64_t)row * B.nx);
         for (int c = 0; c < 4; ++c) {
-            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i) - dense[c * n + i];
+            const double d = state_at(prec, q_hi, q_lo, B.q_off + c * np + i, I.qref[c]) - dense[c * n + i];
             s += d * d * hx[col] * hy[row];
         }
     }
@@ -130,25 +138,18 @@ __global__ void sum_partials_kernel(const double* __restrict__ partials, int npe
     out[j] = s;
 }
 
-__global__ void max_speed_kernel(const BlockDev* __restrict__ blocks, int prec, const void* q_hi,
-                                 const double* __restrict__ met64, unsigned long long* out) {
+__global__ void max_speed_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst, int prec,
+                                 const void* q_hi, const void* q_lo, const double* __restrict__ met64,
+                                 unsigned long long* out) {
     const int b = blockIdx.y;
     const BlockDev& B = blocks[b];
+    const InstanceDev& I = inst[B.instance];
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     double mu = 0.0, mv = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double rho, rhou, rhov;
-        if (prec == 0) {
-            const double* q = static_cast<const double*>(q_hi) + B.q_off;
-            rho = q[i];
-            rhou = q[np + i];
-            rhov = q[2 * np + i];
-        } else {
-            const float* q = static_cast<const float*>(q_hi) + B.q_off;
-            rho = q[i];
-            rhou = q[np + i];
-            rhov = q[2 * np + i];
-        }
+        const double rho = state_at(prec, q_hi, q_lo, B.q_off + i, I.qref[0]);
+        const double rhou = state_at(prec, q_hi, q_lo, B.q_off + np + i, I.qref[1]);
+        const double rhov = state_at(prec, q_hi, q_lo, B.q_off + 2 * np + i, I.qref[2]);
         const double* m = met64 + B.m_off;
         const double u = rhou / rho, v = rhov / rho;
         const double uhat = m[np + i] * u + m[2 * np + i] * v;
@@ -189,40 +190,38 @@ __global__ void time_update_kernel(InstanceDev* inst, const int* __restrict__ ac
     if (i < ninst && active[i]) inst[i].time = inst[i].time + inst[i].dt;
 }
 
-__global__ void pack_kernel(const BlockDev* __restrict__ blocks, const int64_t* __restrict__ poff, int prec,
-                            int dtype, const void* q_hi, const void* q_lo, void* packed) {
+__global__ void pack_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst,
+                            const int64_t* __restrict__ poff, int prec, int dtype, const void* q_hi, const void* q_lo,
+                            void* packed) {
     const BlockDev& B = blocks[blockIdx.y];
+    const InstanceDev& I = inst[B.instance];
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     const int64_t o = poff[blockIdx.y];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         for (int c = 0; c < 4; ++c) {
-            const int64_t g = B.q_off + c * np + i;
+            const double v = state_at(prec, q_hi, q_lo, B.q_off + c * np + i, I.qref[c]);
             if (dtype == 0) {
-                static_cast<double*>(packed)[o + c * n + i] = state_at(prec, q_hi, q_lo, g);
+                static_cast<double*>(packed)[o + c * n + i] = v;
             } else {
                 float* p = static_cast<float*>(packed) + o;
-                if (prec == 0) {
-                    float h, l;
-                    split_f32(static_cast<const double*>(q_hi)[g], h, l);
-                    p[c * n + i] = h;
-                    p[4 * n + c * n + i] = l;
-                } else {
-                    p[c * n + i] = static_cast<const float*>(q_hi)[g];
-                    p[4 * n + c * n + i] = static_cast<const float*>(q_lo)[g];
-                }
+                float h, l;
+                split_f32(v, h, l);
+                p[c * n + i] = h;
+                p[4 * n + c * n + i] = l;
             }
         }
     }
 }
 
-__global__ void unpack_kernel(const BlockDev* __restrict__ blocks, const int64_t* __restrict__ poff, int prec,
-                              int dtype, const void* packed, void* q_hi, void* q_lo) {
+__global__ void unpack_kernel(const BlockDev* __restrict__ blocks, const InstanceDev* __restrict__ inst,
+                              const int64_t* __restrict__ poff, int prec, int dtype, const void* packed, void* q_hi,
+                              void* q_lo) {
     const BlockDev& B = blocks[blockIdx.y];
+    const InstanceDev& I = inst[B.instance];
     const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     const int64_t o = poff[blockIdx.y];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         for (int c = 0; c < 4; ++c) {
-            const int64_t g = B.q_off + c * np + i;
             double v;
             if (dtype == 0) {
                 v = static_cast<const double*>(packed)[o + c * n + i];
@@ -230,20 +229,37 @@ __global__ void unpack_kernel(const BlockDev* __restrict__ blocks, const int64_t
                 const float* p = static_cast<const float*>(packed) + o;
                 v = double(p[c * n + i]) + double(p[4 * n + c * n + i]);
             }
-            if (prec == 0) {
-                static_cast<double*>(q_hi)[g] = v;
-            } else if (dtype == 1) {
-                const float* p = static_cast<const float*>(packed) + o;
-                static_cast<float*>(q_hi)[g] = p[c * n + i];
-                static_cast<float*>(q_lo)[g] = p[4 * n + c * n + i];
-            } else {
-                float h, l;
-                split_f32(v, h, l);
-                static_cast<float*>(q_hi)[g] = h;
-                static_cast<float*>(q_lo)[g] = l;
-            }
+            store_state(prec, q_hi, q_lo, B.q_off + c * np + i, v, I.qref[c]);
         }
     }
+}
+
+// alpha_u and alpha_v of the compensated form's reference state on one block's metrics
+// (upwind_dissipation, euler/src/lib.rs:619-674, at q = q_r), with the metrics rounded to f32
+// as the stage kernels read them, into dense (ny, nx) planes.
+__global__ void alpha_ref_kernel(const BlockDev* __restrict__ blk, const InstanceDev* __restrict__ inst, double gamma,
+                                 const double* __restrict__ met64, double* __restrict__ au, double* __restrict__ av) {
+    const BlockDev& B = *blk;
+    const InstanceDev& I = inst[B.instance];
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
+    const double* m = met64 + B.m_off;
+    const double ur = double(I.ref.u), vr = double(I.ref.v), cr = double(I.ref.c);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double jxx = float(m[np + i]), jxy = float(m[2 * np + i]);
+        const double jyx = float(m[3 * np + i]), jyy = float(m[4 * np + i]);
+        au[i] = fabs(jxx * ur + jxy * vr) + cr * sqrt(jxx * jxx + jxy * jxy);
+        av[i] = fabs(jyx * ur + jyy * vr) + cr * sqrt(jyx * jyx + jyy * jyy);
+    }
+}
+
+// rinf = (diss_xi(alpha_u,r) + diss_eta(alpha_v,r)) / detJ, narrowed to f32, at the block's r_off.
+__global__ void rinf_kernel(const BlockDev* __restrict__ blk, const double* __restrict__ met64,
+                            const double* __restrict__ dxi, const double* __restrict__ deta, float* __restrict__ rinf) {
+    const BlockDev& B = *blk;
+    const int64_t n = (int64_t)B.nx * B.ny;
+    const double* detj = met64 + B.m_off;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        rinf[B.r_off + i] = float((dxi[i] + deta[i]) / detj[i]);
 }
 
 dim3 per_block_grid(int nblocks, int64_t max_points) {
@@ -297,18 +313,19 @@ cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nbl
     return cudaGetLastError();
 }
 
-cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
-                       const double* hx, const double* hy, int64_t max_points, double* sum, double* partials,
-                       cudaStream_t st) {
+cudaError_t diff_terms(const BlockDev* block, const InstanceDev* inst, int prec, const void* q_hi, const void* q_lo,
+                       const double* dense, const double* hx, const double* hy, int64_t max_points, double* sum,
+                       double* partials, cudaStream_t st) {
     const dim3 g = norm_grid(1, max_points);
-    diff_kernel<<<g.x, kT, 0, st>>>(block, prec, q_hi, q_lo, dense, hx, hy, partials);
+    diff_kernel<<<g.x, kT, 0, st>>>(block, inst, prec, q_hi, q_lo, dense, hx, hy, partials);
     sum_partials_kernel<<<1, 32, 0, st>>>(partials, (int)g.x, 1, sum);
     return cudaGetLastError();
 }
 
-cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
-                       int64_t max_points, unsigned long long* out2, cudaStream_t st) {
-    max_speed_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, prec, q_hi, met64, out2);
+cudaError_t max_speeds(const BlockDev* blocks, const InstanceDev* inst, int nblocks, int prec, const void* q_hi,
+                       const void* q_lo, const double* met64, int64_t max_points, unsigned long long* out2,
+                       cudaStream_t st) {
+    max_speed_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, prec, q_hi, q_lo, met64, out2);
     return cudaGetLastError();
 }
 
@@ -318,22 +335,41 @@ cudaError_t combine_stages(const BlockDev* blocks, const InstanceDev* inst, int 
     return cudaGetLastError();
 }
 
+cudaError_t free_stream_dissipation(const BlockDev* block, const InstanceDev* inst, double gamma, int op_xi,
+                                    int op_eta, int nx, int ny, const double* met64, double* work, float* rinf,
+                                    cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny;
+    double* au = work;
+    double* av = work + n;
+    double* dxi = work + 2 * n;
+    double* deta = work + 3 * n;
+    alpha_ref_kernel<<<flat_grid(n), kT, 0, st>>>(block, inst, gamma, met64, au, av);
+    cudaError_t e = cudaGetLastError();
+    e = e ?: op_apply(op_xi, 0, 1, 0, au, dxi, ny, nx, 1, n, st);
+    e = e ?: op_apply(op_eta, 1, 1, 0, av, deta, ny, nx, 1, n, st);
+    if (e != cudaSuccess) return e;
+    rinf_kernel<<<flat_grid(n), kT, 0, st>>>(block, met64, dxi, deta, rinf);
+    return cudaGetLastError();
+}
+
 cudaError_t time_update(InstanceDev* inst, const int* active, int ninst, cudaStream_t st) {
     time_update_kernel<<<(ninst + kT - 1) / kT, kT, 0, st>>>(inst, active, ninst);
     return cudaGetLastError();
 }
 
-cudaError_t pack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
-                       const void* q_hi, const void* q_lo, void* packed, int64_t max_points, cudaStream_t st) {
-    pack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, packed_off, prec, dtype, q_hi, q_lo,
-                                                                   packed);
+cudaError_t pack_state(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const int64_t* packed_off,
+                       int prec, int dtype, const void* q_hi, const void* q_lo, void* packed, int64_t max_points,
+                       cudaStream_t st) {
+    pack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, packed_off, prec, dtype, q_hi,
+                                                                   q_lo, packed);
     return cudaGetLastError();
 }
 
-cudaError_t unpack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
-                         const void* packed, void* q_hi, void* q_lo, int64_t max_points, cudaStream_t st) {
-    unpack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, packed_off, prec, dtype, packed, q_hi,
-                                                                     q_lo);
+cudaError_t unpack_state(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const int64_t* packed_off,
+                         int prec, int dtype, const void* packed, void* q_hi, void* q_lo, int64_t max_points,
+                         cudaStream_t st) {
+    unpack_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, inst, packed_off, prec, dtype, packed,
+                                                                     q_hi, q_lo);
     return cudaGetLastError();
 }
 

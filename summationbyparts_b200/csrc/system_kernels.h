@@ -37,13 +37,14 @@ cudaError_t error_terms(const BlockDev* blocks, const InstanceDev* inst, int nbl
 
 // Field::h2_err of one block's state against a dense (4, ny, nx) f64 field: *sum = terms
 // (partials: kNormParts doubles).
-cudaError_t diff_terms(const BlockDev* block, int prec, const void* q_hi, const void* q_lo, const double* dense,
-                       const double* hx, const double* hy, int64_t max_points, double* sum, double* partials,
-                       cudaStream_t st);
+cudaError_t diff_terms(const BlockDev* block, const InstanceDev* inst, int prec, const void* q_hi, const void* q_lo,
+                       const double* dense, const double* hx, const double* hy, int64_t max_points, double* sum,
+                       double* partials, cudaStream_t st);
 
 // max |uhat|, max |vhat| per block (multigrid/src/system.rs:555-580), as ordered bit patterns.
-cudaError_t max_speeds(const BlockDev* blocks, int nblocks, int prec, const void* q_hi, const double* met64,
-                       int64_t max_points, unsigned long long* out2, cudaStream_t st);
+cudaError_t max_speeds(const BlockDev* blocks, const InstanceDev* inst, int nblocks, int prec, const void* q_hi,
+                       const void* q_lo, const double* met64, int64_t max_points, unsigned long long* out2,
+                       cudaStream_t st);
 
 // One explicit Runge-Kutta combination (utils/integrate/src/lib.rs:193-211):
 // out = base; out = out + (coef[j] * dt) * k[j] for j = 0 .. nk-1 with coef[j] != 0, in that
@@ -63,11 +64,24 @@ cudaError_t combine_stages(const BlockDev* blocks, const InstanceDev* inst, int 
 cudaError_t time_update(InstanceDev* inst, const int* active, int ninst, cudaStream_t st);
 
 // Packed host layout (blocks concatenated, each (4, ny, nx) dense) <-> padded device planes.
-// dtype of the packed buffer: 0 = f64 (widened / split to hi+lo for f32 state),
-//                              1 = f32 hi planes followed by lo planes per block.
-cudaError_t pack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
-                       const void* q_hi, const void* q_lo, void* packed, int64_t max_points, cudaStream_t st);
-cudaError_t unpack_state(const BlockDev* blocks, int nblocks, const int64_t* packed_off, int prec, int dtype,
-                         const void* packed, void* q_hi, void* q_lo, int64_t max_points, cudaStream_t st);
+// The packed state is the absolute state; a compensated system's planes hold its deviation from
+// each instance's reference state (InstanceDev::qref), converted in f64.
+// dtype of the packed buffer: 0 = f64,
+//                              1 = f32 hi planes followed by lo planes per block (hi + lo = state).
+cudaError_t pack_state(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const int64_t* packed_off,
+                       int prec, int dtype, const void* q_hi, const void* q_lo, void* packed, int64_t max_points,
+                       cudaStream_t st);
+cudaError_t unpack_state(const BlockDev* blocks, const InstanceDev* inst, int nblocks, const int64_t* packed_off,
+                         int prec, int dtype, const void* packed, void* q_hi, void* q_lo, int64_t max_points,
+                         cudaStream_t st);
+
+// Free-stream dissipation plane of one block of a compensated upwind system:
+// rinf = (diss_xi(alpha_u,r) + diss_eta(alpha_v,r)) / detJ in f64, stored as f32 at the block's
+// r_off, where alpha_u,r / alpha_v,r are the upwind dissipation coefficients at the instance's
+// reference state (euler/src/lib.rs:619-674).  The stage kernels add q_r * rinf to k.
+// `work` holds 4 nx ny doubles.
+cudaError_t free_stream_dissipation(const BlockDev* block, const InstanceDev* inst, double gamma, int op_xi,
+                                    int op_eta, int nx, int ny, const double* met64, double* work, float* rinf,
+                                    cudaStream_t st);
 
 }  // namespace sbp
