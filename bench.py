@@ -168,6 +168,20 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows), "source": self.source}
 
 
+OP_NAMES = {0: "Upwind4", 1: "Upwind4h2", 2: "Upwind9", 3: "Upwind9h2", 4: "SBP4", 5: "SBP8"}
+
+
+def group_schedule(sysx) -> list:
+    """The tile schedule of every operator group (the autotuner's choice, or the fixed one)."""
+    out = []
+    for g, (ox, oy, pts) in enumerate(sysx.groups()):
+        ty, cps, grid = sysx.group_tiles(g)
+        out.append({"op_xi": OP_NAMES.get(ox, ox), "op_eta": OP_NAMES.get(oy, oy), "points": pts, "tile_rows": ty,
+                    "tile_cols": 32, "ctas_per_sm": "max" if cps < 0 else ("one per tile" if cps == 0 else cps),
+                    "grid": grid})
+    return out
+
+
 def measured_hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -387,7 +401,7 @@ def run_ours(args):
             s64.advance(1)
         ms64 = sharding.max_over_ranks(timed_advance(torch, s64, stream, args.steps, barrier), dist if world > 1 else None)
         v64 = total_points * args.steps / (ms64 / 1e3)
-        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "tiles": list(t64),
+        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "tiles": group_schedule(s64),
                 "bytes_per_point_update": BYTES_PER_POINT_UPDATE["f64"],
                 "achieved_gbs": BYTES_PER_POINT_UPDATE["f64"] * points / (ms64 / args.steps / 1e3) / 1e9,
                 "speedup_f32_over_f64": value / v64}
@@ -498,7 +512,7 @@ def run_ours(args):
                 "config": {"workload": "batched ensemble: 512 vortex solves per GPU (SplitMix64 seed 1), sides 48-257, "
                                        "Upwind4/Upwind9 50/50, warped single blocks, vortex SATs, FP32 compensated RK4",
                            "instances_per_gpu": len(insts), "points_per_gpu": points, "precision": "f32c",
-                           "tiles": list(tiles), "l2": f"inputs larger than L2 (state+metrics "
+                           "tiles": group_schedule(s32), "l2": f"inputs larger than L2 (state+metrics "
                                                        f"{points * 4 * (8 + 8 + 4 + 4 + 5) / 1e6:.0f} MB per GPU)",
                            "parallelism": f"ensemble sharded, {world} rank(s), no collective"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,

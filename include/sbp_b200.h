@@ -262,10 +262,17 @@ sbp_status sbp_system_error(sbp_system* sys, double* per_instance);
 sbp_status sbp_system_h2_err(sbp_system* sys, int block, const double* q, double* err);
 
 /* Tile schedule: output tiles of ty x tx points per CTA, `threads` threads per CTA
- * (0 = keep).  sbp_system_autotune times the candidate schedules on the current state
- * (state and time are restored) and keeps the fastest. */
+ * (0 = keep), for every operator group; clears the autotuner's per-group choices.
+ * sbp_system_autotune searches, per operator group, the tile rows (16, 32) and the width of the
+ * stage kernel's grid (as many persistent CTAs per SM as fit, one per SM, or one CTA per tile),
+ * timing whole RK4 steps on the current state (state and time are restored) by coordinate
+ * descent over the groups, and keeps the fastest; it returns the tile shape of the group with
+ * the most points. */
 sbp_status sbp_system_set_tiles(sbp_system* sys, int ty, int tx, int threads);
 sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads);
+/* Schedule of one operator group: tile rows, persistent CTAs per SM (-1 = as many as fit,
+ * 0 = one CTA per tile) and the resulting grid size of its stage kernel. */
+sbp_status sbp_system_group_tiles(sbp_system* sys, int group, int* ty, int* ctas_per_sm, int* grid);
 
 /* Stream the system launches on (cudaStream_t as void*; NULL = a stream owned by the system). */
 sbp_status sbp_system_set_stream(sbp_system* sys, void* stream);

@@ -88,6 +88,7 @@ SIGNATURES = {
     "sbp_system_h2_err": (_i, [_vp, _i, _dp, _dp]),
     "sbp_system_set_tiles": (_i, [_vp, _i, _i, _i]),
     "sbp_system_autotune": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "sbp_system_group_tiles": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sbp_system_set_stream": (_i, [_vp, _vp]),
     "sbp_system_device_state": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
     "sbp_system_launches_per_step": (_i, [_vp]),

@@ -94,8 +94,18 @@ struct Group {
     double* d_evz = nullptr;  // SBP_BC_EVAL data of those edge points (systems with such sides)
     int64_t points = 0;       // grid points of the group's blocks
     int WX = 0, HY = 0;
+    int ty = 16;              // tile rows
+    int ctas = -1;            // persistent CTAs per SM (-1: as many as fit), 0: one CTA per tile
     size_t smem = 0;
     int grid = 0;
+};
+
+// Tile schedule chosen for one operator group (set by the autotuner): tile rows and the width
+// of the stage kernel's grid.
+struct TileChoice {
+    int opx, opy;
+    bool upw;
+    int ty, ctas;
 };
 
 // One chunk of sbp_system_advance_host: the blocks [b0, b1) (whole instances), their own step
@@ -158,6 +168,8 @@ struct sbp_system {
     int kbuf_stages = 0;
     // schedule
     int TY = 16, TX = kTileX, threads = kStageThreads;
+    std::vector<TileChoice> tile_choice;  // per operator group; groups not listed use (TY, -1)
+    int tiles_gen = 0;                    // bumped whenever the tile schedule changes
     std::vector<int> active;
     std::vector<Group> groups;
     bool sched_dirty = true;
@@ -172,7 +184,7 @@ struct sbp_system {
     // chunk schedules of sbp_system_advance_host, valid for the tile shape and form they were
     // built with
     std::vector<Chunk> chunks;
-    int chunk_ty = 0, chunk_req = 0;
+    int chunk_gen = -1, chunk_req = 0;
     bool chunk_trad = false;
 
     cudaStream_t st() const { return has_user_stream ? user_stream : stream; }
@@ -458,7 +470,7 @@ const Tableau* tableau_of(int id) {
 sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const int* d_active,
                             std::vector<Group>& groups, cudaGraph_t& graph_out, cudaGraphExec_t& gexec_out) {
     free_group_list(groups, graph_out, gexec_out);
-    const int TY = s->TY, TX = s->TX;
+    const int TX = s->TX;
     for (int b = 0; b < s->nblocks; ++b) {
         const BlockDev& B = s->hb[b];
         if (!active[B.instance]) continue;
@@ -474,7 +486,13 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             g.opx = B.op_xi;
             g.opy = B.op_eta;
             g.upw = upw;
-            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw, TY);
+            g.ty = s->TY;
+            for (const TileChoice& c : s->tile_choice)
+                if (c.opx == g.opx && c.opy == g.opy && c.upw == g.upw) {
+                    g.ty = c.ty;
+                    g.ctas = c.ctas;
+                }
+            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw, g.ty);
             if (!g.fn) {
                 set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", B.op_xi, B.op_eta);
                 return SBP_ERR_UNSUPPORTED;
@@ -495,6 +513,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
         for (; gi < groups.size(); ++gi)
             if (groups[gi].opx == B.op_xi && groups[gi].opy == B.op_eta && groups[gi].upw == upw) break;
         Group& g = groups[gi];
+        const int TY = g.ty;
         for (int y0 = 0; y0 < B.ny; y0 += TY)
             for (int x0 = 0; x0 < B.nx; x0 += TX) {
                 int lo, hi;
@@ -513,6 +532,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
     }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         Group& g = groups[gi];
+        const int TY = g.ty;
         g.ntiles = (int)tiles[gi].size();
         g.smem = stage_smem_host(s->prec, g.opx, g.opy, g.upw, TY);
         {
@@ -538,7 +558,9 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
                       g.smem);
             return SBP_ERR_INVALID_ARGUMENT;
         }
-        g.grid = std::min(g.ntiles, per_sm * s->num_sms);
+        // persistent grid of up to `ctas` CTAs per SM, or one CTA per tile (ctas == 0)
+        const int cps = g.ctas < 0 ? per_sm : std::min(g.ctas, per_sm);
+        g.grid = g.ctas == 0 ? g.ntiles : std::min(g.ntiles, cps * s->num_sms);
         if (g.ntiles) {
             SBP_TRY_CUDA(cudaMalloc(&g.d_tiles, g.ntiles * sizeof(int4)));
             SBP_TRY_CUDA(cudaMemcpyAsync(g.d_tiles, tiles[gi].data(), g.ntiles * sizeof(int4),
@@ -1288,7 +1310,7 @@ sbp_status build_chunks(sbp_system* s, int want) {
                                      s->stream));
         SBP_TRY(build_step_graph(s, ch.active, ch.d_active, ch.groups, ch.graph, ch.gexec));
     }
-    s->chunk_ty = s->TY;
+    s->chunk_gen = s->tiles_gen;
     s->chunk_trad = s->force_trad;
     s->chunk_req = want;
     return SBP_OK;
@@ -1309,7 +1331,8 @@ sbp_status sbp_system_advance_host(sbp_system* sys, int dtype, const void* q_in,
         }
     SBP_TRY(check_eval(sys));
     const int want = nchunks > 0 ? std::min(nchunks, 64) : 16;
-    if (sys->chunks.empty() || sys->chunk_req != want || sys->chunk_ty != sys->TY || sys->chunk_trad != sys->force_trad)
+    if (sys->chunks.empty() || sys->chunk_req != want || sys->chunk_gen != sys->tiles_gen ||
+        sys->chunk_trad != sys->force_trad)
         SBP_TRY(build_chunks(sys, want));
     cudaStream_t st = sys->st();
     const int64_t* poff = dtype == SBP_F64 ? sys->d_poff4 : sys->d_poff8;
@@ -1503,6 +1526,8 @@ sbp_status sbp_system_set_tiles(sbp_system* sys, int ty, int tx, int threads) {
     sys->TY = ty;
     sys->TX = tx;
     sys->threads = kStageThreads;
+    sys->tile_choice.clear();
+    ++sys->tiles_gen;
     sys->sched_dirty = true;
     return SBP_OK;
 }
@@ -1517,76 +1542,123 @@ sbp_status sbp_system_autotune(sbp_system* sys, int* ty, int* tx, int* threads) 
             return SBP_ERR_INVALID_ARGUMENT;
         }
     std::fill(sys->active.begin(), sys->active.end(), 1);
-    static const int cand[][3] = {{16, kTileX, kStageThreads}, {32, kTileX, kStageThreads}};
     const size_t ts = sys->tsize();
-    // save state and times; the copies are freed on every return path
+    // save state and times; the copies and events are released on every return path
     struct Saved {
         void* hi = nullptr;
         void* lo = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
         ~Saved() {
             if (hi) cudaFree(hi);
             if (lo) cudaFree(lo);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
         }
     } saved;
     SBP_TRY_CUDA(cudaMalloc(&saved.hi, sys->nq * ts));
     if (sys->prev_lo) SBP_TRY_CUDA(cudaMalloc(&saved.lo, sys->nq * ts));
-    void* const save_hi = saved.hi;
-    void* const save_lo = saved.lo;
+    SBP_TRY_CUDA(cudaEventCreate(&saved.e0));
+    SBP_TRY_CUDA(cudaEventCreate(&saved.e1));
     cudaStream_t st = sys->st();
     SBP_TRY(sync_times(sys));
     std::vector<InstanceDev> save_inst = sys->hi;
-    cudaMemcpyAsync(save_hi, sys->prev_hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
-    if (save_lo) cudaMemcpyAsync(save_lo, sys->prev_lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    float best = 1e30f;
-    int bi = -1;
-    const int oTY = sys->TY, oTX = sys->TX, oth = sys->threads;
-    for (int c = 0; c < (int)(sizeof cand / sizeof cand[0]); ++c) {
-        sys->TY = cand[c][0];
-        sys->TX = cand[c][1];
-        sys->threads = cand[c][2];
+    SBP_TRY_CUDA(cudaMemcpyAsync(saved.hi, sys->prev_hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st));
+    if (saved.lo) SBP_TRY_CUDA(cudaMemcpyAsync(saved.lo, sys->prev_lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st));
+
+    // One RK4 step of the whole schedule (every group, the groups running concurrently as in
+    // production), median of a few replays after a warm-up replay; infinite if it cannot run.
+    auto time_step = [&]() -> float {
+        ++sys->tiles_gen;
         sys->sched_dirty = true;
-        if (build_schedule(sys) != SBP_OK) continue;
-        if (run_steps(sys, 1) != SBP_OK) continue;
-        const int reps = 3;
-        cudaEventRecord(e0, st);
-        if (run_steps(sys, reps) != SBP_OK) continue;
-        cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) {
-            best = ms;
-            bi = c;
+        if (build_schedule(sys) != SBP_OK || run_steps(sys, 1) != SBP_OK) {
+            clear_error();
+            return 1e30f;
         }
+        std::vector<float> t;
+        for (int r = 0; r < 5; ++r) {
+            cudaEventRecord(saved.e0, st);
+            if (run_steps(sys, 1) != SBP_OK) {
+                clear_error();
+                return 1e30f;
+            }
+            cudaEventRecord(saved.e1, st);
+            cudaEventSynchronize(saved.e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, saved.e0, saved.e1);
+            t.push_back(ms);
+        }
+        std::sort(t.begin(), t.end());
+        return t[t.size() / 2];
+    };
+    // the operator groups of the schedule
+    SBP_TRY(build_schedule(sys));
+    std::vector<TileChoice> choice;
+    for (const Group& g : sys->groups) choice.push_back(TileChoice{g.opx, g.opy, g.upw, g.ty, g.ctas});
+    // Candidates per group: tile rows {16, 32} x grid {as many CTAs per SM as fit, one per SM,
+    // one CTA per tile}; coordinate descent over the groups (each group's choice timed with the
+    // others at their current choice), two sweeps.
+    static const int kCand[][2] = {{16, -1}, {32, -1}, {16, 1}, {32, 1}, {16, 0}, {32, 0}};
+    sys->tile_choice = choice;
+    float best = time_step();
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        bool changed = false;
+        for (size_t gi = 0; gi < choice.size(); ++gi) {
+            for (const auto& c : kCand) {
+                if (choice[gi].ty == c[0] && choice[gi].ctas == c[1]) continue;
+                std::vector<TileChoice> trial = choice;
+                trial[gi].ty = c[0];
+                trial[gi].ctas = c[1];
+                sys->tile_choice = trial;
+                const float ms = time_step();
+                if (ms < 0.99f * best) {  // keep a change only for a clear gain
+                    best = ms;
+                    choice = trial;
+                    changed = true;
+                }
+            }
+        }
+        if (!changed) break;
     }
+    sys->tile_choice = choice;
+    ++sys->tiles_gen;
+    sys->sched_dirty = true;
     // restore
-    cudaMemcpyAsync(sys->prev_hi, save_hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
-    if (save_lo) cudaMemcpyAsync(sys->prev_lo, save_lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st);
+    SBP_TRY_CUDA(cudaMemcpyAsync(sys->prev_hi, saved.hi, sys->nq * ts, cudaMemcpyDeviceToDevice, st));
+    if (saved.lo) SBP_TRY_CUDA(cudaMemcpyAsync(sys->prev_lo, saved.lo, sys->nq * ts, cudaMemcpyDeviceToDevice, st));
     sys->hi = save_inst;
-    upload_instances(sys);
-    cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st);
-    cudaStreamSynchronize(st);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    SBP_TRY(upload_instances(sys));
+    SBP_TRY_CUDA(cudaMemsetAsync(sys->status, 0, sizeof(unsigned), st));
+    SBP_TRY_CUDA(cudaStreamSynchronize(st));
     clear_error();
-    if (bi < 0) {
-        sys->TY = oTY;
-        sys->TX = oTX;
-        sys->threads = oth;
-        sys->sched_dirty = true;
+    if (!(best < 1e29f)) {
         set_error("no tile candidate could run");
         return SBP_ERR_CUDA;
     }
-    sys->TY = cand[bi][0];
-    sys->TX = cand[bi][1];
-    sys->threads = cand[bi][2];
-    sys->sched_dirty = true;
-    if (ty) *ty = sys->TY;
+    // the tile rows of the group with the most points
+    int64_t most = -1;
+    int ty_main = sys->TY;
+    SBP_TRY(build_schedule(sys));
+    for (const Group& g : sys->groups)
+        if (g.points > most) {
+            most = g.points;
+            ty_main = g.ty;
+        }
+    if (ty) *ty = ty_main;
     if (tx) *tx = sys->TX;
     if (threads) *threads = sys->threads;
+    return SBP_OK;
+}
+
+sbp_status sbp_system_group_tiles(sbp_system* sys, int group, int* ty, int* ctas_per_sm, int* grid) {
+    clear_error();
+    if (!sys) return SBP_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(sys->device);
+    if (sys->sched_dirty) SBP_TRY(build_schedule(sys));
+    if (group < 0 || group >= (int)sys->groups.size()) return SBP_ERR_INVALID_ARGUMENT;
+    const Group& g = sys->groups[group];
+    if (ty) *ty = g.ty;
+    if (ctas_per_sm) *ctas_per_sm = g.ctas;
+    if (grid) *grid = g.grid;
     return SBP_OK;
 }
 

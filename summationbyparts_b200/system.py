@@ -177,6 +177,13 @@ class BlockSystem:
             out.append((ox.value, oy.value, pts.value))
         return out
 
+    def group_tiles(self, group: int) -> tuple[int, int, int]:
+        """(tile rows, persistent CTAs per SM (-1 = as many as fit, 0 = one CTA per tile), grid
+        size) of one stage-kernel group's schedule."""
+        ty, cps, grid = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(_capi.lib.sbp_system_group_tiles(self.h, group, ctypes.byref(ty), ctypes.byref(cps), ctypes.byref(grid)))
+        return ty.value, cps.value, grid.value
+
     def launch_stage(self, group: int, stage: int, with_edges: bool = False) -> None:
         """Enqueue one group's stage kernel (and optionally its edge kernel) on the system's
         stream.  Advances no time; the stage buffers are left as the launch leaves them."""

@@ -98,21 +98,27 @@ def test_config0_vortex_100_steps(orc):
 
 
 def test_multiblock_interfaces(orc):
-    """Configuration 2 layout (6 curvilinear Upwind9 blocks, Grid interfaces, vortex outer edges)."""
+    """Configuration 2 layout (6 curvilinear Upwind9 blocks, Grid interfaces, vortex outer edges),
+    the configured 500 RK4 steps: f64 within 1e-12 of the oracle, the compensated form within
+    1e-6 of it (the six listed block sizes admit no layout under the reference's couplings,
+    tests/test_config2_layout_cpu.py; this is the conforming 2 x 3 layout)."""
     from summationbyparts_b200 import workloads
     blocks = workloads.multiblock()
     dt = workloads.multiblock_dt(blocks)
     o = oracle_system(orc, blocks, workloads.STANDARD_VORTEX)
     o.init_vortex(0.0)
-    g = gpu_system(blocks, workloads.STANDARD_VORTEX)
-    for b in range(len(blocks)):
-        g.set_state(b, o.state(b))
-    g.set_dt(dt)
-    g.advance(25)
-    o.advance(25, dt)
-    for b in range(len(blocks)):
-        assert rel_l2(g.state(b), o.state(b)) <= PARITY, b
-    assert abs(g.errors()[0] - o.error()) <= 1e-10 * o.error()
+    q0 = [o.state(b) for b in range(len(blocks))]
+    o.advance(500, dt)
+    for prec, bar in (("f64", PARITY), ("f32c", 1e-6)):
+        g = gpu_system(blocks, workloads.STANDARD_VORTEX, prec)
+        for b in range(len(blocks)):
+            g.set_state(b, q0[b])
+        g.set_dt(dt)
+        g.advance(500)
+        for b in range(len(blocks)):
+            assert rel_l2(g.state(b), o.state(b)) <= bar, (prec, b)
+        assert abs(g.errors()[0] - o.error()) <= (1e-10 if prec == "f64" else 1e-3) * o.error()
+        g.close()
 
 
 def test_max_dt_bitwise(orc):
