@@ -221,6 +221,7 @@ struct sbp_cnn {
     float* y = nullptr;               // output [B][kPix][8]
     __nv_bfloat16* dz[kLayers] = {};  // output gradients
     float *part_w = nullptr, *part_b = nullptr, *part_loss = nullptr;
+    unsigned* status = nullptr;       // device status word of the tensor-core kernels
     float4 in_mean{0, 0, 0, 0}, in_inv{1, 1, 1, 1}, out_scale{1, 1, 1, 1};
     int adam_t = 0;
     std::vector<void*> allocs;
@@ -232,8 +233,29 @@ namespace {
 template <int CIN, int COUT, int EPI>
 cudaError_t conv(const sbp_cnn* c, int n, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
                  const float* zprev, float* zout, __nv_bfloat16* yout) {
-    conv3x3_kernel<CIN, COUT, EPI><<<n * (kImg / kBand), kConvThreads, 0, c->st()>>>(x, w, bias, zprev, zout, yout);
+    constexpr int bytes = ConvTcLayout<CIN, COUT>::BYTES;
+    static bool configured = false;  // per instantiation; the attribute is per function
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT, EPI>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    conv3x3_tc_kernel<CIN, COUT, EPI><<<n * (kImg / kBand), kConvThreads, bytes, c->st()>>>(x, w, bias, zprev, zout,
+                                                                                            yout, c->status);
     return cudaGetLastError();
+}
+
+// The device status word after the stream has drained: a tensor-core wait that gave up.
+sbp_status device_status(sbp_cnn* c) {
+    unsigned h = 0;
+    SBP_TRY_CUDA(cudaMemcpyAsync(&h, c->status, sizeof h, cudaMemcpyDeviceToHost, c->st()));
+    SBP_TRY_CUDA(cudaStreamSynchronize(c->st()));
+    if (h & kStatusMmaTimeout) {
+        set_error("a convolution's tensor-core work did not complete in time");
+        return SBP_ERR_CUDA;
+    }
+    return SBP_OK;
 }
 
 template <int CIN, int M, int MSTORE>
@@ -297,7 +319,7 @@ sbp_status backward(sbp_cnn* c, int n, const void* coarse, int dtype, int64_t im
     if (loss) {
         std::vector<float> h(blocks);
         SBP_TRY_CUDA(cudaMemcpyAsync(h.data(), c->part_loss, blocks * sizeof(float), cudaMemcpyDeviceToHost, c->st()));
-        SBP_TRY_CUDA(cudaStreamSynchronize(c->st()));
+        SBP_TRY(device_status(c));
         double s = 0.0;
         for (float v : h) s += v;
         *loss = float(s / double(total * 4));
@@ -369,6 +391,7 @@ sbp_status sbp_cnn_create(int device, int max_batch, unsigned long long seed, sb
     e = e ?: alloc((void**)&c->part_w, B * (kImg / kWgradRows) * (32 * 9 * 32) * 4);
     e = e ?: alloc((void**)&c->part_b, B * (kImg / kWgradRows) * 32 * 4);
     e = e ?: alloc((void**)&c->part_loss, (B * kPix + 255) / 256 * 4);
+    e = e ?: alloc((void**)&c->status, sizeof(unsigned));
     if (e != cudaSuccess) return fail(cuda_status(e, "network allocation"));
     // He-style initialisation for the GELU layers, a small output layer so the initial
     // correction is close to zero; padded entries stay zero.
@@ -481,7 +504,7 @@ sbp_status sbp_cnn_gradients(sbp_cnn* c, int n, const void* d_coarse, int dtype,
     SBP_TRY(backward(c, n, d_coarse, dtype, img_stride, d_fine_r, loss));
     if (host_grads) {
         SBP_TRY_CUDA(cudaMemcpyAsync(host_grads, c->G, c->nparams * 4, cudaMemcpyDeviceToHost, c->st()));
-        SBP_TRY_CUDA(cudaStreamSynchronize(c->st()));
+        SBP_TRY(device_status(c));
     }
     return SBP_OK;
 }
@@ -527,7 +550,7 @@ sbp_status sbp_cnn_synchronize(sbp_cnn* c) {
     clear_error();
     if (!c) return SBP_ERR_INVALID_ARGUMENT;
     SBP_TRY_CUDA(cudaStreamSynchronize(c->st()));
-    return SBP_OK;
+    return device_status(c);
 }
 
 sbp_status sbp_restrict_linspace(int n, int nf, int nc, const double* d_fine, double* d_coarse, void* stream) {

@@ -1,7 +1,9 @@
 // Kernels of the learned correction network: a 5-layer 3x3 convolutional network on the 64 x 64
 // coarse grid (4 -> 32 -> 32 -> 32 -> 32 -> 4 channels, GELU between layers).  Activations are
-// BF16 in NHWC layout (channels innermost), accumulation is FP32 on the tensor cores
-// (mma.sync m16n8k16 bf16), pre-activations, outputs, gradients and parameters are FP32.
+// BF16 in NHWC layout (channels innermost), accumulation is FP32 on the tensor cores:
+// the convolutions (forward and backward-data) on tcgen05 with TMEM accumulators, the weight
+// gradients on warp-level mma.sync m16n8k16 (their GEMM has only 16-32 output-channel rows,
+// below tcgen05's minimum M of 64); pre-activations, outputs, gradients and parameters are FP32.
 //
 // Channel counts are padded to what one MMA step consumes: the 4-channel input is stored with
 // 16 channels (zeros above 4), the 4-channel output with 8, and the gradient of the output with
@@ -52,103 +54,231 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const unsigned*>(&v);
 }
 
-// 3x3 convolution with zero padding as an implicit GEMM: out[p][n] = sum over taps t and input
-// channels k of x[p + off(t)][k] * w[n][t][k], off(t) = (t / 3 - 1, t % 3 - 1).  One CTA takes
-// kBand image rows: their halo (kBand + 2 rows x 66 columns) and all weights go to shared
-// memory, warp w computes 32 pixels of row w / 2 for all COUT channels.  Epilogues:
+// ---- tcgen05 (5th-generation tensor core) helpers, sm_100a --------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor of a K-major bf16 operand in the canonical layout without
+// swizzling: core matrices of 8 rows x 16 bytes (128 contiguous bytes, row after row), adjacent
+// core matrices `lbo` bytes apart along K and `sbo` bytes apart along M (or N).  Fields: start
+// address / 16 (bits 0-13), lbo / 16 (16-29), sbo / 16 (32-45), descriptor version 1 (46-47),
+// base offset 0, layout type 0 = no swizzle (61-63).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16 with bf16 A and B (both K-major) and an f32
+// accumulator, M x N: D format (bits 4-5) = f32, A and B formats (7-9, 10-12) = bf16, N / 8
+// (17-22), M / 16 (24-28).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D (tmem) = A * B (+ D when accumulate != 0), issued by one thread.
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// Arrive on the mbarrier once every tcgen05.mma issued so far by this thread has completed.
+__device__ __forceinline__ void umma_commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\nselp.b32 %0, 1, 0, q;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(mbar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive f32 TMEM columns of this thread's lane (32x32b shape: warp w reads lanes
+// 32 w .. 32 w + 31, so the lane field of taddr must be 32 w).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+        "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Bit of the network's device status word set when a convolution gave up waiting for its
+// tensor-core work (the wait is bounded, so a fault cannot hang the stream).
+constexpr unsigned kStatusMmaTimeout = 1u;
+constexpr int kMmaWaitLimit = 1 << 22;  // mbarrier polls before giving up
+
+// Shared-memory layout of the tcgen05 convolution (dynamic, 1024-byte aligned base).
+template <int CIN, int COUT>
+struct ConvTcLayout {
+    static constexpr int NP = COUT < 16 ? 16 : COUT;        // N of the MMA (multiple of 16 for M = 128)
+    static constexpr int HR = kBand + 2;                    // halo rows
+    static constexpr int PIX = HR * kImg;                   // pixels of one shifted copy
+    static constexpr int CH = CIN / 8;                      // 16-byte channel chunks per pixel
+    static constexpr int SBO = CH * 128;                    // bytes between 8-row groups
+    static constexpr int A_BYTES = PIX * CIN * 2;           // one shifted copy
+    static constexpr int B_TAP = NP * CIN * 2;              // weights of one tap
+    static constexpr int B_OFF = 3 * A_BYTES;
+    static constexpr int BAR_OFF = B_OFF + 9 * B_TAP;
+    static constexpr int BYTES = BAR_OFF + 16;
+};
+// Byte offset of (row, 16-byte chunk kc) in a canonical no-swizzle K-major operand.
+template <int CH>
+__device__ __forceinline__ int canon_off(int row, int kc) {
+    return ((row >> 3) * CH + kc) * 128 + (row & 7) * 16;
+}
+
+// 3x3 convolution with zero padding as an implicit GEMM on the tcgen05 tensor cores:
+// out[p][n] = sum over taps t and input channels k of x[p + off(t)][k] * w[n][t][k],
+// off(t) = (t / 3 - 1, t % 3 - 1).  One CTA of 128 threads computes kBand = 2 image rows
+// (M = 128 pixels) for all output channels (N = COUT, at least 16): the input halo goes to
+// shared memory as three copies shifted by 0, 1 and 2 columns, each in the canonical K-major
+// layout, so the A operand of tap (dy, dx) is copy dx started dy image rows down -- an aligned
+// descriptor offset, no per-tap copy; the weights of the 9 taps follow in the same layout.  One
+// thread issues the 9 * CIN / 16 MMAs (K = 16 each) into a TMEM accumulator of 128 lanes x N
+// f32 columns and commits them to an mbarrier; after the (bounded) wait each warp reads its 32
+// lanes -- one pixel per thread, all channels -- and runs the epilogue:
 //   EPI_GELU   z = acc + bias -> zout (f32), gelu(z) -> yout (bf16)   (hidden layers)
 //   EPI_LINEAR acc + bias -> zout (f32)                                (output layer)
 //   EPI_DGELU  acc * gelu'(zprev) -> yout (bf16)                       (gradient of a hidden layer)
-// Shared rows are padded by 8 bf16 so the fragment loads of 8 consecutive pixels (or output
-// channels) fall in distinct banks.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(const __nv_bfloat16* __restrict__ x,
-                                                               const __nv_bfloat16* __restrict__ w,
-                                                               const float* __restrict__ bias,
-                                                               const float* __restrict__ zprev,
-                                                               float* __restrict__ zout,
-                                                               __nv_bfloat16* __restrict__ yout) {
-    static_assert(CIN % 16 == 0 && COUT % 8 == 0, "channel padding");
-    constexpr int SP = CIN + 8;
-    constexpr int HR = kBand + 2, HC = kImg + 2;
-    constexpr int NT = COUT / 8;
-    __shared__ __align__(16) __nv_bfloat16 sx[HR * HC * SP];
-    __shared__ __align__(16) __nv_bfloat16 sw[COUT * 9 * SP];
+__global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                  const __nv_bfloat16* __restrict__ w,
+                                                                  const float* __restrict__ bias,
+                                                                  const float* __restrict__ zprev,
+                                                                  float* __restrict__ zout,
+                                                                  __nv_bfloat16* __restrict__ yout,
+                                                                  unsigned* __restrict__ status) {
+    using L = ConvTcLayout<CIN, COUT>;
+    static_assert(CIN % 16 == 0 && COUT % 8 == 0 && L::NP <= 32, "channel padding");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8);
     const int img = blockIdx.x / (kImg / kBand);
     const int r0 = (blockIdx.x % (kImg / kBand)) * kBand;
-    for (int i = threadIdx.x; i < COUT * 9 * (CIN / 8); i += kConvThreads) {
-        const int row = i / (CIN / 8), v = i % (CIN / 8);
-        *reinterpret_cast<uint4*>(sw + row * SP + v * 8) = *reinterpret_cast<const uint4*>(w + row * CIN + v * 8);
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (warp == 0) {
+        // 32 TMEM columns (the allocation minimum) hold the 128 x NP f32 accumulator
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < HR * HC * (CIN / 8); i += kConvThreads) {
-        const int pix = i / (CIN / 8), v = i % (CIN / 8);
-        const int hr = pix / HC, hc = pix % HC;
+    if (tid == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // weights: B[n][k] of tap t = w[n][t][k], rows n >= COUT zero
+    for (int i = tid; i < L::NP * 9 * L::CH; i += kConvThreads) {
+        const int kc = i % L::CH, t = (i / L::CH) % 9, n = i / (L::CH * 9);
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (n < COUT) v = *reinterpret_cast<const uint4*>(w + ((int64_t)n * 9 + t) * CIN + kc * 8);
+        *reinterpret_cast<uint4*>(smem + L::B_OFF + t * L::B_TAP + canon_off<L::CH>(n, kc)) = v;
+    }
+    // input halo: rows r0 - 1 .. r0 + kBand, columns -1 .. 64 (zero outside the image), into the
+    // copies shifted by dx: copy dx, pixel (hr, c) = halo (hr, c + dx)
+    for (int i = tid; i < L::HR * (kImg + 2) * L::CH; i += kConvThreads) {
+        const int kc = i % L::CH, hc = (i / L::CH) % (kImg + 2), hr = i / (L::CH * (kImg + 2));
         const int gr = r0 + hr - 1, gc = hc - 1;
-        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
         if (gr >= 0 && gr < kImg && gc >= 0 && gc < kImg)
-            val = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + v * 8);
-        *reinterpret_cast<uint4*>(sx + pix * SP + v * 8) = val;
+            v = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + kc * 8);
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+            const int c = hc - dx;
+            if (c >= 0 && c < kImg)
+                *reinterpret_cast<uint4*>(smem + dx * L::A_BYTES + canon_off<L::CH>(hr * kImg + c, kc)) = v;
+        }
     }
+    // the operands written through the generic proxy become visible to the tensor core's proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wr = warp >> 1, wc0 = (warp & 1) * 32;
-    const int g = lane >> 2, q = lane & 3;
-    float acc[2][NT][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0f;
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    if (tid == 0) {
+        constexpr uint32_t idesc = umma_idesc_bf16(128, L::NP);
+        const uint32_t base = smem_u32(smem);
+        uint32_t acc = 0;
 #pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3, dx = tap % 3;
+        for (int t = 0; t < 9; ++t) {
+            const int dy = t / 3, dx = t % 3;
 #pragma unroll
-        for (int c0 = 0; c0 < CIN; c0 += 16) {
-            unsigned a[2][4];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const __nv_bfloat16* p0 = sx + ((wr + dy) * HC + wc0 + mt * 16 + g + dx) * SP + c0 + 2 * q;
-                const __nv_bfloat16* p1 = p0 + 8 * SP;
-                a[mt][0] = *reinterpret_cast<const unsigned*>(p0);
-                a[mt][1] = *reinterpret_cast<const unsigned*>(p1);
-                a[mt][2] = *reinterpret_cast<const unsigned*>(p0 + 8);
-                a[mt][3] = *reinterpret_cast<const unsigned*>(p1 + 8);
-            }
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const __nv_bfloat16* pb = sw + ((nt * 8 + g) * 9 + tap) * SP + c0 + 2 * q;
-                const unsigned b[2] = {*reinterpret_cast<const unsigned*>(pb),
-                                       *reinterpret_cast<const unsigned*>(pb + 8)};
-                mma_bf16(acc[0][nt], a[0], b);
-                mma_bf16(acc[1][nt], a[1], b);
+            for (int j = 0; j < CIN / 16; ++j) {
+                const uint32_t a = base + dx * L::A_BYTES + dy * (kImg / 8) * L::SBO + 2 * j * 128;
+                const uint32_t b = base + L::B_OFF + t * L::B_TAP + 2 * j * 128;
+                umma_bf16(tmem, umma_desc(a, 128, L::SBO), umma_desc(b, 128, L::SBO), idesc, acc);
+                acc = 1;
             }
         }
+        umma_commit(mbar);
     }
-    const int row = r0 + wr;
+    bool done = false;
+    for (int it = 0; it < kMmaWaitLimit && !done; ++it) done = mbar_try_wait(mbar, 0);
+    tc_fence_after();
+    if (done) {
+        // thread tid holds accumulator row tid: pixel (r0 + tid / 64, tid % 64)
+        const int64_t p = (int64_t)(img * kImg + r0 + tid / kImg) * kImg + tid % kImg;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        float v[32];
+        if constexpr (L::NP == 32) tmem_ld32(taddr, v);
+        else tmem_ld16(taddr, v);
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int col = wc0 + mt * 16 + g + half * 8;
-            const int64_t p = (int64_t)(img * kImg + row) * kImg + col;
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const int co = nt * 8 + 2 * q;
-                const float v0 = acc[mt][nt][2 * half], v1 = acc[mt][nt][2 * half + 1];
-                if constexpr (EPI == EPI_GELU) {
-                    const float z0 = v0 + bias[co], z1 = v1 + bias[co + 1];
-                    *reinterpret_cast<float2*>(zout + p * COUT + co) = make_float2(z0, z1);
-                    *reinterpret_cast<unsigned*>(yout + p * COUT + co) = pack_bf16(gelu(z0), gelu(z1));
-                } else if constexpr (EPI == EPI_LINEAR) {
-                    *reinterpret_cast<float2*>(zout + p * COUT + co) = make_float2(v0 + bias[co], v1 + bias[co + 1]);
-                } else {
-                    const float2 zp = *reinterpret_cast<const float2*>(zprev + p * COUT + co);
-                    *reinterpret_cast<unsigned*>(yout + p * COUT + co) =
-                        pack_bf16(v0 * gelu_grad(zp.x), v1 * gelu_grad(zp.y));
-                }
+        for (int co = 0; co < COUT; co += 2) {
+            const float v0 = v[co], v1 = v[co + 1];
+            if constexpr (EPI == EPI_GELU) {
+                const float z0 = v0 + bias[co], z1 = v1 + bias[co + 1];
+                *reinterpret_cast<float2*>(zout + p * COUT + co) = make_float2(z0, z1);
+                *reinterpret_cast<unsigned*>(yout + p * COUT + co) = pack_bf16(gelu(z0), gelu(z1));
+            } else if constexpr (EPI == EPI_LINEAR) {
+                *reinterpret_cast<float2*>(zout + p * COUT + co) = make_float2(v0 + bias[co], v1 + bias[co + 1]);
+            } else {
+                const float2 zp = *reinterpret_cast<const float2*>(zprev + p * COUT + co);
+                *reinterpret_cast<unsigned*>(yout + p * COUT + co) = pack_bf16(v0 * gelu_grad(zp.x), v1 * gelu_grad(zp.y));
             }
         }
+    } else if ((tid & 31) == 0) {
+        atomicOr(status, kStatusMmaTimeout);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+    }
 }
 
 // Weight and bias gradients of one layer: dw[m][t][k] = sum over pixels p of dz[p][m] *
