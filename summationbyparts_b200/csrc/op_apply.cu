@@ -3,6 +3,15 @@
 // Compiled with -fmad=false: results are bit-identical to the reference's row path
 // (xi) and column path (eta) in the same dtype.
 //
+// Aligned arrays (rows and batch stride multiples of 16 bytes, 16-byte aligned base pointers)
+// take the bulk-staged kernels: one tile per CTA, every input row segment of the tile (with its
+// halo or closure region) brought into shared memory by one cp.async.bulk copy that completes
+// on an mbarrier, so a CTA has its whole tile in flight at once and no thread spends
+// instructions on the loads.  Row tiles: kXiBulkRows rows x 128 vectors of 16 bytes (256 f64 or
+// 512 f32 outputs per row), each thread one 16-byte output vector per row.  Column tiles:
+// kEtaBulkRows rows x 1 KB of adjacent columns, each thread one column over its share of the
+// rows with the D-tap window in a register ring.  Other arrays take the kernels below.
+//
 // Row direction: a CTA stages kXiRows row segments (plus halo) in shared memory, with 16-byte
 // loads when the rows are 16-byte aligned; each thread
 // then reads its window with 16-byte vector loads and produces 16/sizeof(T) consecutive
@@ -19,6 +28,7 @@
 
 #include <cstdint>
 
+#include "bulk_copy.cuh"
 #include "op_apply.h"
 #include "sbp_ops.cuh"
 
@@ -233,6 +243,158 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+constexpr int kBulkWait = 1 << 22;  // mbarrier polls before a tile gives up
+// Tiles whose staged rows did not arrive within kBulkWait polls; their outputs are not written.
+__device__ unsigned g_bulk_timeouts = 0;
+
+constexpr int kXiBulkRows = 16;
+template <class T>
+constexpr int xi_bulk_cols() { return 128 * (16 / (int)sizeof(T)); }
+template <class T>
+constexpr int xi_bulk_pitch() { return xi_bulk_cols<T>() + 32; }  // covers the halo, closures and alignment
+template <class T>
+constexpr size_t xi_bulk_smem() { return (size_t)kXiBulkRows * xi_bulk_pitch<T>() * sizeof(T) + 16; }
+
+// Row direction, bulk-staged tile (see the file comment).  Requires nx and bstride multiples of
+// K = 16 / sizeof(T) and 16-byte aligned arrays.
+template <int OP, int KIND, class T>
+__global__ void __launch_bounds__(kThreads)
+    op_xi_bulk_kernel(const T* __restrict__ in, T* __restrict__ out, int ny, int nx, int64_t bstride, T idx) {
+    constexpr int M = OpShape<OP>::M, H = OpShape<OP>::H;
+    constexpr int K = 16 / sizeof(T);
+    constexpr int TC = xi_bulk_cols<T>(), P = xi_bulk_pitch<T>(), TR = kXiBulkRows;
+    constexpr int PAD = ((H + K - 1) / K) * K;
+    constexpr int NV = (K + 2 * PAD) / K;
+    using V = typename Vec<T>::type;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)TR * P * sizeof(T));
+    const int ncb = (nx + TC - 1) / TC, nrg = (ny + TR - 1) / TR;
+    int64_t it = blockIdx.x;
+    const int cb = (int)(it % ncb);
+    it /= ncb;
+    const int rg = (int)(it % nrg);
+    const int64_t b = it / nrg;
+    const int c0 = cb * TC, c1 = min(nx, c0 + TC);
+    const int y0 = rg * TR, nrows = min(TR, ny - y0);
+    int lo, hi;
+    region_of<OP>(c0, c1, nx, lo, hi);
+    lo -= lo % K;                              // 16-byte aligned segment start
+    hi = min(nx, (hi + K - 1) / K * K);        // and a whole number of 16-byte vectors
+    const uint32_t row_bytes = (uint32_t)(hi - lo) * (uint32_t)sizeof(T);
+    const T* src = in + b * bstride + (int64_t)y0 * nx + lo;
+    if (threadIdx.x == 0) bulk_mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) bulk_expect(bar, row_bytes * (uint32_t)nrows);
+        for (int r = threadIdx.x; r < nrows; r += 32) bulk_g2s(buf + r * P, src + (int64_t)r * nx, row_bytes, bar);
+    }
+    if (!bulk_wait(bar, 0, kBulkWait)) {
+        if (threadIdx.x == 0) atomicAdd(&g_bulk_timeouts, 1u);
+        return;
+    }
+    const int sub = threadIdx.x / 128, v = threadIdx.x % 128;
+    const int c = c0 + K * v;  // first of this thread's K outputs; buf column 0 is input column lo
+    if (c >= c1) return;
+    const bool interior = c >= M && c + K - 1 < nx - M;
+    for (int r = sub; r < nrows; r += 2) {
+        const T* rb = buf + r * P;
+        T* dst = out + b * bstride + (int64_t)(y0 + r) * nx;
+        T o[K];
+        if (interior) {
+            T w[K + 2 * PAD];  // w[j] holds column c - PAD + j
+            const V* bv = reinterpret_cast<const V*>(rb + (c - PAD - lo));
+#pragma unroll
+            for (int q = 0; q < NV; ++q) reinterpret_cast<V*>(w)[q] = bv[q];
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                o[j] = diag_unfused<OP, KIND, T>([&](int d) { return w[j + d + PAD - H]; }) * idx;
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                o[j] = sum_unfused<OP, KIND, T>(c + j, nx, [&](int kk) { return rb[kk - lo]; }) * idx;
+        }
+        *reinterpret_cast<V*>(dst + c) = *reinterpret_cast<V*>(o);
+    }
+}
+
+constexpr int kEtaBulkRows = 48;
+template <int OP, class T>
+constexpr int eta_bulk_region() {  // input rows a column tile can need (region_of's extent)
+    constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N, H = OpShape<OP>::H;
+    constexpr int a = kEtaBulkRows + H + (H > M - 1 ? H : M - 1);
+    return a > N ? a : N;
+}
+template <int OP, class T>
+constexpr size_t eta_bulk_smem() { return (size_t)eta_bulk_region<OP, T>() * 1024 + 16; }
+
+// Column direction, bulk-staged tile (see the file comment).  Same requirements as the row tile.
+template <int OP, int KIND, class T>
+__global__ void __launch_bounds__(kThreads)
+    op_eta_bulk_kernel(const T* __restrict__ in, T* __restrict__ out, int ny, int nx, int64_t bstride, T idx,
+                       int simd) {
+    constexpr int M = OpShape<OP>::M, D = OpShape<OP>::D, H = OpShape<OP>::H;
+    constexpr int TC = 1024 / sizeof(T), TR = kEtaBulkRows;
+    constexpr int GROUPS = kThreads / TC;  // row groups (2 in f64, 1 in f32)
+    constexpr int RG = TR / GROUPS;        // rows of one thread
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)eta_bulk_region<OP, T>() * 1024);
+    const int ncb = (nx + TC - 1) / TC, nrc = (ny + TR - 1) / TR;
+    int64_t it = blockIdx.x;  // vertically adjacent tiles are adjacent in launch order (shared halos in L2)
+    const int rc = (int)(it % nrc);
+    it /= nrc;
+    const int cb = (int)(it % ncb);
+    const int64_t b = it / ncb;
+    const int y0 = rc * TR, y1 = min(ny, y0 + TR), c0 = cb * TC, tw = min(TC, nx - c0);
+    int lo, hi;
+    region_of<OP>(y0, y1, ny, lo, hi);
+    const int nrows = hi - lo;
+    const uint32_t row_bytes = (uint32_t)tw * (uint32_t)sizeof(T);
+    const T* src = in + b * bstride + (int64_t)lo * nx + c0;
+    if (threadIdx.x == 0) bulk_mbar_init(bar, 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) bulk_expect(bar, row_bytes * (uint32_t)nrows);
+        for (int r = threadIdx.x; r < nrows; r += 32) bulk_g2s(buf + r * TC, src + (int64_t)r * nx, row_bytes, bar);
+    }
+    if (!bulk_wait(bar, 0, kBulkWait)) {
+        if (threadIdx.x == 0) atomicAdd(&g_bulk_timeouts, 1u);
+        return;
+    }
+    const int j = threadIdx.x % TC, g = threadIdx.x / TC;
+    if (j >= tw) return;
+    const int col = c0 + j;
+    const bool fused = col < simd;
+    T* dst = out + b * bstride + col;
+    auto at = [&](int r) { return buf[(r - lo) * TC + j]; };
+    const int ra = y0 + g * RG, rb = min(y1, ra + RG);
+    for (int r = ra; r < rb && r < M; ++r) dst[(int64_t)r * nx] = sum_column<OP, KIND, T>(fused, r, ny, at) * idx;
+    for (int r = max(ra, ny - M); r < rb; ++r) dst[(int64_t)r * nx] = sum_column<OP, KIND, T>(fused, r, ny, at) * idx;
+    const int i0 = max(ra, M), i1 = min(rb, ny - M);
+    if (i0 >= i1) return;
+    T w[D];
+#pragma unroll
+    for (int k = 0; k < D - 1; ++k) w[k] = at(i0 - H + k);
+    int r = i0;
+    for (; r + D <= i1; r += D) {
+#pragma unroll
+        for (int u = 0; u < D; ++u) {
+            w[(u + D - 1) % D] = at(r + u + H);
+            T f = T(0);
+            if (fused) {
+#pragma unroll
+                for (int k = 0; k < D; ++k) f = fma_rn(w[(u + k) % D], Coef<OP, KIND, T>::diag(k), f);
+            } else {
+#pragma unroll
+                for (int k = 0; k < D; ++k) f = f + Coef<OP, KIND, T>::diag(k) * w[(u + k) % D];
+            }
+            dst[(int64_t)(r + u) * nx] = f * idx;
+        }
+    }
+    for (; r < i1; ++r) dst[(int64_t)r * nx] = sum_column<OP, KIND, T>(fused, r, ny, at) * idx;
+}
+
 int g_num_sms = 0;
 
 int num_sms() {
@@ -253,9 +415,37 @@ cudaError_t launch_t(int dir, const T* in, T* out, int64_t ny, int64_t nx, int64
     // throughput prefers to a persistent grid that loops load -> compute -> store.
     const int blocks_cap = 1 << 30;
     (void)num_sms;
+    constexpr int K = 16 / sizeof(T);
+    const bool aligned = (nx % K == 0) && (bstride % K == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) &&
+                         (reinterpret_cast<uintptr_t>(out) % 16 == 0);
+    if (aligned) {
+        // bulk-staged tiles, one per CTA
+        if (dir == 0) {
+            const T idx = inv_spacing<T>(OpShape<OP>::h2, nx);
+            constexpr int TC = xi_bulk_cols<T>();
+            const int64_t items = nbatch * ((ny + kXiBulkRows - 1) / kXiBulkRows) * ((nx + TC - 1) / TC);
+            op_xi_bulk_kernel<OP, KIND, T><<<(unsigned)items, kThreads, xi_bulk_smem<T>(), st>>>(
+                in, out, (int)ny, (int)nx, bstride, idx);
+        } else {
+            const T idx = inv_spacing<T>(OpShape<OP>::h2, ny);
+            const int simd = (int)(simd_lanes<T>() * (nx / simd_lanes<T>()));
+            constexpr int TC = 1024 / sizeof(T);
+            constexpr size_t smem = eta_bulk_smem<OP, T>();
+            static bool configured = false;  // per instantiation: the attribute belongs to the function
+            if (!configured) {
+                const cudaError_t e = cudaFuncSetAttribute(op_eta_bulk_kernel<OP, KIND, T>,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+                configured = true;
+            }
+            const int64_t items = nbatch * ((ny + kEtaBulkRows - 1) / kEtaBulkRows) * ((nx + TC - 1) / TC);
+            op_eta_bulk_kernel<OP, KIND, T><<<(unsigned)items, kThreads, smem, st>>>(in, out, (int)ny, (int)nx, bstride,
+                                                                                     idx, simd);
+        }
+        return cudaGetLastError();
+    }
     if (dir == 0) {
         const T idx = inv_spacing<T>(OpShape<OP>::h2, nx);
-        constexpr int K = 16 / sizeof(T);
         const int64_t nseg = (nx + kThreads * K - 1) / (kThreads * K);
         const int64_t items = nbatch * ((ny + kXiRows - 1) / kXiRows) * nseg;
         const int grid = (int)(items < blocks_cap ? items : blocks_cap);
