@@ -47,7 +47,8 @@ __host__ __device__ constexpr int64_t edge_count(int64_t nx, int64_t ny) { retur
 
 // Reference state of the compensated-f32 form, as f32 constants of the deviation arithmetic:
 // the conserved state q_r = (rho_r, m_r, n_r, e_r), velocity (u_r, v_r), pressure p_r,
-// total enthalpy H_r = e_r + p_r, sound speed c_r and c_r^2, gamma / rho_r.
+// total enthalpy H_r = e_r + p_r, sound speed c_r and c_r^2, gamma / rho_r.  It is always the
+// reference's vortex free stream (rho_r = 1, u_r = 1, v_r = 0), which the stage kernels use.
 struct RefState {
     float q[4];
     float u, v, p, h, c, c2, g_rho;

@@ -278,33 +278,36 @@ __device__ __forceinline__ void pointwise(const T qv[4], const T m[4], T gamma, 
 //   u H - u_r H_r = du H_r + u dH,  c^2 - c_r^2 = (gamma / rho_r) (dp rho_r - p_r d0) / rho,
 //   c - c_r = (c^2 - c_r^2) / (c + c_r),  |uhat| - |uhat_r| = sign(uhat_r) duhat when both have
 //   one sign (else the plain difference, whose operands are then no larger than duhat).
+// The reference state is the free stream of the reference's vortex (rho_r = 1, u_r = 1,
+// v_r = 0, so m_r = 1 and n_r = 0; only e_r, p_r and c_r vary with the Mach number), which
+// removes the terms of m_r, n_r and v_r from the algebra above.
 template <bool UPW>
 __device__ __forceinline__ void pointwise_dev(const float d[4], const float m[4], float gamma, const RefState& R,
                                               float* sxi, int xa, float* seta, int ya, bool want_xi, bool want_eta,
                                               unsigned& bad) {
-    const float rho = R.q[0] + d[0];
+    const float rho = 1.0f + d[0];
     const float ri = 1.0f / rho;
-    const float du = (d[1] - R.u * d[0]) * ri, dv = (d[2] - R.v * d[0]) * ri;
-    const float u = R.u + du, v = R.v + dv;
-    const float dmu = R.q[1] * du + d[1] * u;
-    const float dnv = R.q[2] * dv + d[2] * v;
-    const float dmv = R.q[1] * dv + d[1] * v;
+    const float du = (d[1] - d[0]) * ri, v = d[2] * ri;  // u - 1 and v
+    const float u = 1.0f + du;
+    const float dmu = du + d[1] * u;  // m u - 1
+    const float dnv = d[2] * v;       // n v
+    const float mv = v + d[1] * v;    // m v
     const float dp = (gamma - 1.0f) * (d[3] - 0.5f * (dmu + dnv));
     const float dh = d[3] + dp;
     float E[4], F[4];
     E[0] = d[1];
     E[1] = dmu + dp;
-    E[2] = dmv;
+    E[2] = mv;
     E[3] = du * R.h + u * dh;
     F[0] = d[2];
-    F[1] = dmv;
+    F[1] = mv;
     F[2] = dnv + dp;
-    F[3] = dv * R.h + v * dh;
+    F[3] = v * (R.h + dh);
     float c = 0.0f, dc = 0.0f;
     if constexpr (UPW) {
         if (!(rho > 0.0f)) bad |= STATUS_RHO;
         if (!(R.p + dp > 0.0f)) bad |= STATUS_P;
-        const float dc2 = R.g_rho * (dp * R.q[0] - R.p * d[0]) * ri;
+        const float dc2 = gamma * (dp - R.p * d[0]) * ri;  // c^2 - c_r^2 with rho_r = 1
         c = sqrtf(R.c2 + dc2);
         dc = dc2 / (c + R.c);
     }
@@ -312,16 +315,17 @@ __device__ __forceinline__ void pointwise_dev(const float d[4], const float m[4]
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) dst[cc * stride] = jx * E[cc] + jy * F[cc];
         if constexpr (UPW) {
-            const float hr = jx * R.u + jy * R.v;  // uhat at q_r
-            const float dhat = jx * du + jy * dv;
-            const float hat = hr + dhat;
-            const float dabs = hat * hr > 0.0f ? (hr > 0.0f ? dhat : -dhat) : fabsf(hat) - fabsf(hr);
+            const float dhat = jx * du + jy * v;  // uhat - uhat_r, uhat_r = jx
+            const float hat = jx + dhat;
+            const float dabs = hat * jx > 0.0f ? (jx > 0.0f ? dhat : -dhat) : fabsf(hat) - fabsf(jx);
             const float s = sqrtf(jx * jx + jy * jy);
             const float a = fabsf(hat) + c * s;
             const float da = dabs + dc * s;
             float* o = dst + 4 * stride;
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) o[cc * stride] = a * d[cc] + da * R.q[cc];
+            o[0] = a * d[0] + da;  // q_r = (1, 1, 0, e_r)
+            o[stride] = a * d[1] + da;
+            o[2 * stride] = a * d[2];
+            o[3 * stride] = a * d[3] + da * R.q[3];
         }
     };
     if (want_xi) store(m[0], m[1], sxi, xa);
