@@ -304,9 +304,8 @@ sbp_status sbp_system_advance_tableau(sbp_system* sys, int tableau, int64_t nste
  * not advanced (the reference's euler::System has none). */
 sbp_status sbp_system_advance_adaptive(sbp_system* sys, double dt, double* guess_dt, double maxerr);
 
-/* Kernel launches per RK4 step: per operator pair and stage one stage kernel (whose CTAs also
- * apply the SATs of the block-edge points of their tiles), preceded by the expression-data kernel
- * in systems with SBP_BC_EVAL sides, plus the time update. */
+/* Kernel launches per RK4 step: per operator pair and stage a stage kernel and an edge (SAT)
+ * kernel, plus the time update. */
 int sbp_system_launches_per_step(const sbp_system* sys);
 
 /* Per-kernel measurement.  A system's blocks are scheduled in groups, one per operator pair
@@ -317,11 +316,10 @@ int sbp_system_launches_per_step(const sbp_system* sys);
 int sbp_system_group_count(sbp_system* sys);
 /* Operator pair and grid points of one group. */
 sbp_status sbp_system_group_info(sbp_system* sys, int group, int* op_xi, int* op_eta, int64_t* points);
-/* Enqueue one group's stage kernel for RK4 stage 0..3 on the system's stream (SATs of the edge
- * points included; with_edges is ignored, it remains for callers built against the earlier
- * interface).  This advances no time and checks no status: it runs the stage on whatever the
- * stage buffers hold, so a system used for it must be re-initialised before its results mean
- * anything. */
+/* Enqueue one group's stage kernel for RK4 stage 0..3 on the system's stream, followed by its
+ * edge (SAT) kernel when with_edges != 0.  This advances no time and checks no status: it runs
+ * the stage on whatever the stage buffers hold, so a system used for it must be re-initialised
+ * before its results mean anything. */
 sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int with_edges);
 
 /* ---------------------------------------------------------------------------------------

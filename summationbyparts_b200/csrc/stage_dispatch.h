@@ -20,6 +20,9 @@ const void* stage_ptr_f64_xsa(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f64_xsb(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_x49(int opx, int opy, bool upw, int ty);
 const void* stage_ptr_f32_xs(int opx, int opy, bool upw, int ty);
+// Edge (SAT) kernel entries, one per precision.
+const void* sat_ptr_f64();
+const void* sat_ptr_f32();
 // Expression-boundary (SBP_BC_EVAL) data kernel entries, one per precision.
 const void* eval_ptr_f64();
 const void* eval_ptr_f32();

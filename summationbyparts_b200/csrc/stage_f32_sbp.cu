@@ -1,5 +1,4 @@
-// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs, and of the expression-boundary data
-// kernel, compensated f32 state.
+// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs and of the edge (SAT) kernel, compensated f32 state.
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
 #include "stage_kernel_vec.cuh"
@@ -21,6 +20,7 @@ const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty) {
     return nullptr;
 }
 
+const void* sat_ptr_f32() { return reinterpret_cast<const void*>(&sat_kernel<float, true>); }
 const void* eval_ptr_f32() { return reinterpret_cast<const void*>(&eval_kernel<float>); }
 
 }  // namespace sbp

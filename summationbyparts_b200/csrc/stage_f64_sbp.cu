@@ -1,5 +1,4 @@
-// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs, and of the expression-boundary data
-// kernel, f64 state (reference arithmetic, built with -fmad=false).
+// Instantiations of the fused stage kernel for the SBP4/SBP8 operator pairs and of the edge (SAT) kernel, f64 state (reference arithmetic, built with -fmad=false).
 #include "stage_dispatch.h"
 #include "stage_kernel.cuh"
 
@@ -17,6 +16,7 @@ const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty) {
     return nullptr;
 }
 
+const void* sat_ptr_f64() { return reinterpret_cast<const void*>(&sat_kernel<double, false>); }
 const void* eval_ptr_f64() { return reinterpret_cast<const void*>(&eval_kernel<double>); }
 
 }  // namespace sbp

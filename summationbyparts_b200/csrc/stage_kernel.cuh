@@ -11,13 +11,12 @@
 //   stage 3: new  = acc + (b3 dt) k
 // which is the reference's sequence fut = prev; fut += b_j dt k_j (j = 0..3) evaluated
 // incrementally, so the k_j of interior points never go to memory.  Points on a block edge
-// store their k in the edge-k buffer instead; after its tile loop each CTA adds the
-// characteristic SATs of those points in the order north, south, east, west
-// (SAT_characteristics, euler/src/lib.rs:1002-1013) and does their update (edge_tail).  The SAT
-// of one point is a long dependent f64 chain (vortex data, two hypot, a dozen divisions);
-// evaluated by the few threads of a tile that hold edge points it would hold the whole CTA at the
-// next barrier, so the CTA collects the edge points of all its tiles and deals them to all its
-// threads at once.
+// store their k in the edge-k buffer instead; the edge kernel (sat_kernel, launched right after
+// on the same stream) adds the characteristic SATs in the order north, south, east, west
+// (SAT_characteristics, euler/src/lib.rs:1002-1013) and does their update.  The SAT of one
+// point is a long dependent f64 chain (vortex data, two hypot, a dozen divisions); evaluated by
+// a few threads of a tile it held the whole CTA at the next barrier, in a launch of its own it
+// runs one thread per edge point.
 //
 // Work decomposition.  A persistent grid of 256-thread CTAs walks a list of (block, y0, x0)
 // output tiles of TY rows x 32 columns.  Lane = column, warp w owns rows w*R .. w*R+R-1
@@ -583,8 +582,8 @@ __device__ __forceinline__ double absolute_state(const StageArgs<T>& A, const Bl
 
 // SATs of one block-edge point in the reference's order N, S, E, W; k updated in place.
 template <class T>
-__device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int64_t eslot,
-                                      int row, int col, int pt, const double yv[4], double kv[4]) {
+__device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int eidx, int row,
+                                      int col, int pt, const double yv[4], double kv[4]) {
     const int nx = B.nx, ny = B.ny;
     const int64_t np = B.npad;
     const bool on[4] = {row == ny - 1, row == 0, col == nx - 1, col == 0};
@@ -602,7 +601,7 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
             // BoundaryCharacteristic::Eval (euler/src/lib.rs:853-863): the expressions at the stage
             // time, evaluated for this edge point by eval_kernel just before
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc) zv[cc] = A.evz[4 * eslot + cc];
+            for (int cc = 0; cc < 4; ++cc) zv[cc] = A.evz[4 * (int64_t)eidx + cc];
         } else if (kind == BC_INTERPOLATE || kind == BC_MULTIGRID) {
             // boundary_extract (euler/src/lib.rs:816-846): data from neighbours' opposite edges
             const bool ns_ = d == NORTH || d == SOUTH;
@@ -665,10 +664,6 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         sat_point_rows(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
     }
 }
-
-// SATs and RK update of the block-edge points of a CTA's tiles (defined below).
-template <class T, bool COMP>
-__device__ __forceinline__ void edge_tail(const StageArgs<T>& A, int TY);
 
 template <int OPX, int OPY, class T, bool UPW, bool COMP, int TY>
 __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs<T> A) {
@@ -853,19 +848,24 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         // Every thread is done with this tile's shared arrays before the next tile's phase 1.
         __syncthreads();
     }
-    edge_tail<T, COMP>(A, TY);
     if (bad) atomicOr(A.status, bad);
 }
 
-// SATs and RK update of one block-edge point (row, col) of block B: the characteristic SATs are
-// added to the k the stage kernel stored for the point (edge-k buffer), then the point's stage
-// update runs as for interior points.
+// Edge kernel: one thread per block-edge point of a stage launch's blocks (edges[i] = block,
+// row, col).  Adds the SATs to the k the stage kernel stored and does the point's RK update.
+constexpr int kSatThreads = 128;
 template <class T, bool COMP>
-__device__ __forceinline__ void edge_point_update(const StageArgs<T>& A, const BlockDev& B, int row, int col) {
+__global__ void __launch_bounds__(kSatThreads, 4) sat_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
+                                                          int nedges) {
+    const int i = blockIdx.x * kSatThreads + threadIdx.x;
+    if (i >= nedges) return;
+    const int4 ed = edges[i];
+    const BlockDev& B = A.blocks[ed.x];
     const InstanceDev& I = A.inst[B.instance];
+    const int row = ed.y, col = ed.z;
     const int nx = B.nx, ny = B.ny;
     const int64_t np = B.npad, qoff = B.q_off;
-    const int64_t eslot = B.e_off + edge_index(row, col, nx, ny);
+    const int64_t slot = 4 * (B.e_off + edge_index(row, col, nx, ny));
     const double cb = A.stage < 4 ? I.cb[A.stage] : 0.0;
     const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
     const int pt = row * nx + col;
@@ -876,88 +876,20 @@ __device__ __forceinline__ void edge_point_update(const StageArgs<T>& A, const B
     for (int cc = 0; cc < 4; ++cc) {
         qs[cc] = q[cc * np + pt];
         yv[cc] = absolute_state<T>(A, B, cc, qs[cc]);
-        kv[cc] = double(A.kedge[4 * eslot + cc]);
+        kv[cc] = double(A.kedge[slot + cc]);
     }
-    sat_edge<T>(A, I, B, eslot, row, col, pt, yv, kv);
+    sat_edge<T>(A, I, B, i, row, col, pt, yv, kv);
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, qoff + cc * np + pt, qs[cc], T(kv[cc]), cb, ca);
 }
 
-// Block-edge points of the tile [y0, y1) x [x0, x1): those on the block's first and last rows,
-// then those on its first and last columns without the corner rows.
-__device__ __forceinline__ int tile_edge_count(int y0, int y1, int x0, int x1, int nx, int ny) {
-    const int tw = x1 - x0, rows = max(min(y1, ny - 1) - max(y0, 1), 0);
-    return (y0 == 0 ? tw : 0) + (y1 == ny ? tw : 0) + (x0 == 0 ? rows : 0) + (x1 == nx ? rows : 0);
-}
-__device__ __forceinline__ void tile_edge_point(int e, int y0, int y1, int x0, int x1, int nx, int ny, int& row,
-                                                int& col) {
-    const int tw = x1 - x0;
-    if (y0 == 0) {
-        if (e < tw) {
-            row = 0;
-            col = x0 + e;
-            return;
-        }
-        e -= tw;
-    }
-    if (y1 == ny) {
-        if (e < tw) {
-            row = ny - 1;
-            col = x0 + e;
-            return;
-        }
-        e -= tw;
-    }
-    const int r0 = max(y0, 1), rows = max(min(y1, ny - 1) - r0, 0);
-    if (x0 == 0) {
-        if (e < rows) {
-            row = r0 + e;
-            col = 0;
-            return;
-        }
-        e -= rows;
-    }
-    row = r0 + e;
-    col = nx - 1;
-}
-
-// Edge tail of a persistent stage launch: after its tile loop a CTA applies the SATs and the RK
-// update to the block-edge points of the tiles it processed (their k are in the edge-k buffer,
-// written by this CTA and visible after the loop's last barrier).  The points of all its tiles
-// form one list dealt round-robin to the CTA's threads, one point per thread per round, so the
-// long f64 chains of the SATs (vortex data with exp and pow, two hypot, a dozen divisions) run on
-// every thread at once, and the stage needs no second launch.
-template <class T, bool COMP>
-__device__ __forceinline__ void edge_tail(const StageArgs<T>& A, int TY) {
-    int lead = 0;  // edge points of this CTA's earlier tiles, mod the block size
-    for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
-        const int4 td = A.tiles[t];
-        const BlockDev& B = A.blocks[td.x];
-        const int y0 = td.y, x0 = td.z, y1 = min(y0 + TY, B.ny), x1 = min(x0 + kTileX, B.nx);
-        const int cnt = tile_edge_count(y0, y1, x0, x1, B.nx, B.ny);
-        if (cnt == 0) continue;
-        // thread tid takes the tile's points e with (lead + e) mod blockDim.x == tid
-        int e = (int)threadIdx.x - lead;
-        if (e < 0) e += kStageThreads;
-        for (; e < cnt; e += kStageThreads) {
-            int row, col;
-            tile_edge_point(e, y0, y1, x0, x1, B.nx, B.ny, row, col);
-            edge_point_update<T, COMP>(A, B, row, col);
-        }
-        lead = (lead + cnt) % kStageThreads;
-    }
-}
-
-constexpr int kEvalThreads = 128;
-
 // Expression boundary data (SBP_BC_EVAL sides) of a stage launch's edge points (edges[i] =
-// block, row, col) at the stage time, into evz at each point's edge-k slot; launched before the
-// stage kernel only for systems with such sides, so the stage kernel stays free of the
-// interpreter.
+// block, row, col) at the stage time, into evz[4 i ..]; launched before the edge kernel only for
+// systems with such sides, so the edge kernel itself stays free of the interpreter.
 template <class T>
-__global__ void __launch_bounds__(kEvalThreads) eval_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
+__global__ void __launch_bounds__(kSatThreads) eval_kernel(const StageArgs<T> A, const int4* __restrict__ edges,
                                                            int nedges) {
-    const int i = blockIdx.x * kEvalThreads + threadIdx.x;
+    const int i = blockIdx.x * kSatThreads + threadIdx.x;
     if (i >= nedges) return;
     const int4 ed = edges[i];
     const BlockDev& B = A.blocks[ed.x];
@@ -973,8 +905,7 @@ __global__ void __launch_bounds__(kEvalThreads) eval_kernel(const StageArgs<T> A
     const double* xy = A.xy + B.x_off;
     double z[4];
     eval_state(*A.eval, A.gamma, stime, xy[pt], xy[B.npad + pt], z);
-    const int64_t eslot = B.e_off + edge_index(row, col, B.nx, B.ny);
-    for (int cc = 0; cc < 4; ++cc) A.evz[4 * eslot + cc] = z[cc];
+    for (int cc = 0; cc < 4; ++cc) A.evz[4 * (int64_t)i + cc] = z[cc];
 }
 
 }  // namespace sbp

@@ -399,7 +399,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         // Every thread is done with this tile's shared arrays before the next tile's phase 1.
         __syncthreads();
     }
-    edge_tail<float, true>(A, kVecRows);
     if (bad) atomicOr(A.status, bad);
 }
 

@@ -91,6 +91,7 @@ struct Group {
     int ntiles = 0;
     int4* d_edges = nullptr;  // (block, row, col) of every edge point of the group's blocks
     int nedges = 0;
+    double* d_evz = nullptr;  // SBP_BC_EVAL data of those edge points (systems with such sides)
     int64_t points = 0;       // grid points of the group's blocks
     int WX = 0, HY = 0;
     int ty = 16;              // tile rows
@@ -162,7 +163,6 @@ struct sbp_system {
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
     EvalDev* d_eval = nullptr;  // expression programs of SBP_BC_EVAL sides
-    double* d_evz = nullptr;    // their data at every edge point (4 per edge-k slot), when present
     bool has_eval = false, eval_set = false;
     double* kbuf = nullptr;  // k of the stages of a general tableau (kMaxStages x nq, f64), on demand
     int kbuf_stages = 0;
@@ -197,6 +197,7 @@ void free_group_list(std::vector<Group>& groups, cudaGraph_t& graph, cudaGraphEx
     for (auto& g : groups) {
         cudaFree(g.d_tiles);
         cudaFree(g.d_edges);
+        if (g.d_evz) cudaFree(g.d_evz);
     }
     groups.clear();
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -228,7 +229,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf,    s->d_evz};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -334,34 +335,36 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.kedge = static_cast<T*>(s->kedge);
     a.mg = s->d_mg;
     a.eval = s->d_eval;
-    a.evz = s->d_evz;
+    a.evz = g.d_evz;
     a.gamma = s->gamma;
     a.status = s->status;
     return a;
 }
 
-// One group's stage: the expression-boundary data of its edge points (systems with SBP_BC_EVAL
-// sides), then the stage kernel, whose CTAs also apply the SATs of the edge points of their
-// tiles.
-sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st) {
+sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t st, bool edges_too = true) {
     if (g.ntiles == 0) return SBP_OK;
-    cudaError_t e = cudaSuccess;
-    const dim3 ev_grid((g.nedges + kEvalThreads - 1) / kEvalThreads);
+    cudaError_t e;
+    const void* sat = s->prec == 0 ? sat_ptr_f64() : sat_ptr_f32();
+    const dim3 sat_grid((g.nedges + kSatThreads - 1) / kSatThreads);
     int4* edges = g.d_edges;
     int nedges = g.nedges;
     const void* evk = s->prec == 0 ? eval_ptr_f64() : eval_ptr_f32();
     if (s->prec == 0) {
         StageArgs<double> a = stage_args<double>(s, stage, g);
         void* args[] = {&a};
-        void* eargs[] = {&a, &edges, &nedges};
-        if (s->has_eval) e = cudaLaunchKernel(evk, ev_grid, dim3(kEvalThreads), eargs, 0, st);
-        if (e == cudaSuccess) e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess && edges_too && s->has_eval)
+            e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
+        if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     } else {
         StageArgs<float> a = stage_args<float>(s, stage, g);
         void* args[] = {&a};
-        void* eargs[] = {&a, &edges, &nedges};
-        if (s->has_eval) e = cudaLaunchKernel(evk, ev_grid, dim3(kEvalThreads), eargs, 0, st);
-        if (e == cudaSuccess) e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        void* sargs[] = {&a, &edges, &nedges};
+        if (e == cudaSuccess && edges_too && s->has_eval)
+            e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
+        if (e == cudaSuccess && edges_too) e = cudaLaunchKernel(sat, sat_grid, dim3(kSatThreads), sargs, 0, st);
     }
     return cuda_status(e, "stage kernel launch");
 }
@@ -566,6 +569,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             SBP_TRY_CUDA(cudaMalloc(&g.d_edges, g.nedges * sizeof(int4)));
             SBP_TRY_CUDA(cudaMemcpyAsync(g.d_edges, edges[gi].data(), g.nedges * sizeof(int4),
                                          cudaMemcpyHostToDevice, s->stream));
+            if (s->has_eval) SBP_TRY_CUDA(cudaMalloc(&g.d_evz, (size_t)g.nedges * 4 * sizeof(double)));
         }
     }
     SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
@@ -662,13 +666,15 @@ sbp_status launch_rhs(sbp_system* s, const double* u_in, double* k_out, double c
         a.u_in = u_in;
         a.u_out = k_out;
         void* args[] = {&a};
+        SBP_TRY_CUDA(cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st));
         int4* edges = g.d_edges;
         int nedges = g.nedges;
-        void* eargs[] = {&a, &edges, &nedges};
+        void* sargs[] = {&a, &edges, &nedges};
         if (s->has_eval)
-            SBP_TRY_CUDA(cudaLaunchKernel(eval_ptr_f64(), dim3((g.nedges + kEvalThreads - 1) / kEvalThreads),
-                                          dim3(kEvalThreads), eargs, 0, st));
-        SBP_TRY_CUDA(cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st));
+            SBP_TRY_CUDA(cudaLaunchKernel(eval_ptr_f64(), dim3((g.nedges + kSatThreads - 1) / kSatThreads),
+                                          dim3(kSatThreads), sargs, 0, st));
+        SBP_TRY_CUDA(cudaLaunchKernel(sat_ptr_f64(), dim3((g.nedges + kSatThreads - 1) / kSatThreads),
+                                      dim3(kSatThreads), sargs, 0, st));
     }
     return SBP_OK;
 }
@@ -974,7 +980,6 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
-    if (s->has_eval) e = e ?: alloc((void**)&s->d_evz, 4 * s->nedge * sizeof(double));
     e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
     e = e ?: alloc((void**)&s->d_eval, sizeof(EvalDev));
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
@@ -1791,8 +1796,7 @@ sbp_status sbp_system_launch_stage(sbp_system* sys, int group, int stage, int wi
         set_error("group %d out of range (%d groups)", group, (int)sys->groups.size());
         return SBP_ERR_INVALID_ARGUMENT;
     }
-    (void)with_edges;  // the stage kernel applies the SATs of its edge points itself
-    return launch_group(sys, stage, sys->groups[group], sys->st());
+    return launch_group(sys, stage, sys->groups[group], sys->st(), with_edges != 0);
 }
 
 int sbp_system_launches_per_step(const sbp_system* sys) {
@@ -1805,9 +1809,9 @@ int sbp_system_launches_per_step(const sbp_system* sys) {
             auto p = std::make_pair(B.op_xi, B.op_eta);
             if (std::find(pairs.begin(), pairs.end(), p) == pairs.end()) pairs.push_back(p);
         }
-        return (sys->has_eval ? 8 : 4) * (int)pairs.size() + 1;
+        return 8 * (int)pairs.size() + 1;
     }
-    return (sys->has_eval ? 8 : 4) * (int)sys->groups.size() + 1;
+    return (sys->has_eval ? 12 : 8) * (int)sys->groups.size() + 1;
 }
 
 }  // extern "C"
