@@ -136,6 +136,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16-byte asynchronous global -> shared copy; src_bytes = 0 fills the destination with zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
 // Bit of the network's device status word set when a convolution gave up waiting for its
 // tensor-core work (the wait is bounded, so a fault cannot hang the stream).
 constexpr unsigned kStatusMmaTimeout = 1u;
@@ -201,28 +207,27 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
         mbar_init(mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // weights: B[n][k] of tap t = w[n][t][k], rows n >= COUT zero
+    // Operands by asynchronous 16-byte copies straight into the canonical layout, all of a
+    // thread's copies in flight at once.  Weights: B[n][k] of tap t = w[n][t][k], rows n >= COUT
+    // zero-filled.
     for (int i = tid; i < L::NP * 9 * L::CH; i += kConvThreads) {
         const int kc = i % L::CH, t = (i / L::CH) % 9, n = i / (L::CH * 9);
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (n < COUT) v = *reinterpret_cast<const uint4*>(w + ((int64_t)n * 9 + t) * CIN + kc * 8);
-        *reinterpret_cast<uint4*>(smem + L::B_OFF + t * L::B_TAP + canon_off<L::CH>(n, kc)) = v;
+        const bool in = n < COUT;
+        cp_async16(smem + L::B_OFF + t * L::B_TAP + canon_off<L::CH>(n, kc),
+                   w + ((int64_t)(in ? n : 0) * 9 + t) * CIN + kc * 8, in ? 16u : 0u);
     }
     // input halo: rows r0 - 1 .. r0 + kBand, columns -1 .. 64 (zero outside the image), into the
-    // copies shifted by dx: copy dx, pixel (hr, c) = halo (hr, c + dx)
-    for (int i = tid; i < L::HR * (kImg + 2) * L::CH; i += kConvThreads) {
-        const int kc = i % L::CH, hc = (i / L::CH) % (kImg + 2), hr = i / (L::CH * (kImg + 2));
-        const int gr = r0 + hr - 1, gc = hc - 1;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (gr >= 0 && gr < kImg && gc >= 0 && gc < kImg)
-            v = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + kc * 8);
-#pragma unroll
-        for (int dx = 0; dx < 3; ++dx) {
-            const int c = hc - dx;
-            if (c >= 0 && c < kImg)
-                *reinterpret_cast<uint4*>(smem + dx * L::A_BYTES + canon_off<L::CH>(hr * kImg + c, kc)) = v;
-        }
+    // copies shifted by dx: copy dx, pixel (hr, c) = halo (hr, c + dx), i.e. image column c + dx - 1
+    for (int i = tid; i < 3 * L::HR * kImg * L::CH; i += kConvThreads) {
+        const int kc = i % L::CH, c = (i / L::CH) % kImg, hr = (i / (L::CH * kImg)) % L::HR;
+        const int dx = i / (L::CH * kImg * L::HR);
+        const int gr = r0 + hr - 1, gc = c + dx - 1;
+        const bool in = gr >= 0 && gr < kImg && gc >= 0 && gc < kImg;
+        const int64_t pix = in ? (int64_t)(img * kImg + gr) * kImg + gc : 0;
+        cp_async16(smem + dx * L::A_BYTES + canon_off<L::CH>(hr * kImg + c, kc), x + pix * CIN + kc * 8,
+                   in ? 16u : 0u);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     // the operands written through the generic proxy become visible to the tensor core's proxy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
