@@ -261,7 +261,15 @@ sbp_status device_status(sbp_cnn* c) {
 template <int CIN, int M, int MSTORE>
 cudaError_t wgrad(const sbp_cnn* c, int n, int layer, const __nv_bfloat16* x, const __nv_bfloat16* dz) {
     const int parts = n * (kImg / kWgradRows);
-    wgrad_kernel<CIN, M, MSTORE><<<parts, kWgradThreads, 0, c->st()>>>(x, dz, c->part_w, c->part_b);
+    constexpr int bytes = WgradTcLayout<CIN, M>::BYTES;
+    static bool configured = false;  // per instantiation; the attribute is per function
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(wgrad_tc_kernel<CIN, M, MSTORE>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    wgrad_tc_kernel<CIN, M, MSTORE><<<parts, kConvThreads, bytes, c->st()>>>(x, dz, c->part_w, c->part_b, c->status);
     const int nw = MSTORE * 9 * CIN, nb = MSTORE;
     wgrad_reduce_kernel<<<(nw + nb + 255) / 256, 256, 0, c->st()>>>(c->part_w, c->part_b, parts, nw, nb,
                                                                       c->G + c->w_off[layer], c->G + c->b_off[layer]);

@@ -1,9 +1,8 @@
 // Kernels of the learned correction network: a 5-layer 3x3 convolutional network on the 64 x 64
 // coarse grid (4 -> 32 -> 32 -> 32 -> 32 -> 4 channels, GELU between layers).  Activations are
-// BF16 in NHWC layout (channels innermost), accumulation is FP32 on the tensor cores:
-// the convolutions (forward and backward-data) on tcgen05 with TMEM accumulators, the weight
-// gradients on warp-level mma.sync m16n8k16 (their GEMM has only 16-32 output-channel rows,
-// below tcgen05's minimum M of 64); pre-activations, outputs, gradients and parameters are FP32.
+// BF16 in NHWC layout (channels innermost), accumulation is FP32 on the tcgen05 tensor cores
+// with TMEM accumulators (convolutions forward and backward-data, and the weight gradients);
+// pre-activations, outputs, gradients and parameters are FP32.
 //
 // Channel counts are padded to what one MMA step consumes: the 4-channel input is stored with
 // 16 channels (zeros above 4), the 4-channel output with 8, and the gradient of the output with
@@ -21,27 +20,8 @@ constexpr int kPix = kImg * kImg;  // pixels per image
 constexpr int kBand = 2;           // image rows per CTA in the convolution kernels (128 pixels)
 constexpr int kConvThreads = 128;  // 4 warps, 32 pixels each
 constexpr int kWgradRows = 16;     // image rows per CTA in the weight-gradient kernel
-constexpr int kWgradThreads = 288; // 9 warps, one per filter tap
 
 enum Epilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
-
-// D = A * B + D for one 16x16 (row) by 16x8 (col) bf16 tile with f32 accumulators.
-__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const unsigned b[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// Four transposed 8x8 b16 matrices from shared memory; lane i gives the address of row i % 8
-// of matrix i / 8 (16-byte aligned rows).
-__device__ __forceinline__ void ldsm_x4_trans(unsigned r[4], const void* row_addr) {
-    const unsigned a = (unsigned)__cvta_generic_to_shared(row_addr);
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
 
 // GELU with the Gaussian CDF, x * Phi(x), and its derivative Phi(x) + x * phi(x).
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -286,101 +266,176 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
     }
 }
 
-// Weight and bias gradients of one layer: dw[m][t][k] = sum over pixels p of dz[p][m] *
-// x[p + off(t)][k], db[m] = sum over p of dz[p][m], as partial sums per CTA (kWgradRows image
-// rows each) that wgrad_reduce_kernel adds up in a fixed order.  M = channels of dz as stored
-// (16 or 32), MSTORE = rows of the layer's weight tensor (<= M).  Warp t computes tap t; both
-// GEMM operands are pixel-major in memory and reach the MMA through transposing ldmatrix.
+// 8 x 8 transpose of bf16: in[j] holds 8 channels of pixel j, out[i] 8 pixels of channel i.
+__device__ __forceinline__ void transpose8x8_bf16(const uint4 in[8], uint4 out[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const unsigned sel = (i & 1) ? 0x7632u : 0x5410u;  // high or low halves of word i / 2
+        unsigned w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const unsigned a = (&in[2 * q].x)[i >> 1], b = (&in[2 * q + 1].x)[i >> 1];
+            w[q] = __byte_perm(a, b, sel);
+        }
+        out[i] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// Shared-memory layout of the tcgen05 weight-gradient kernel.
+template <int CIN, int M>
+struct WgradTcLayout {
+    static constexpr int ROWS = 9 * CIN + 1;                // (tap, input channel) rows + the ones row
+    static constexpr int TILES = (ROWS + 127) / 128;        // M = 128 tiles
+    static constexpr int AROWS = TILES * 128;
+    static constexpr int P = kImg;                          // pixels per chunk (one image row)
+    static constexpr int SBO = (P / 8) * 128;               // bytes between 8-row groups
+    static constexpr int A_BYTES = AROWS * P * 2;
+    static constexpr int B_OFF = A_BYTES;
+    static constexpr int BAR_OFF = B_OFF + M * P * 2;
+    static constexpr int BYTES = BAR_OFF + 16;
+    static constexpr int TMEM_COLS = TILES * M <= 32 ? 32 : (TILES * M <= 64 ? 64 : 128);
+};
+
+// Weight and bias gradients of one layer on the tcgen05 tensor cores, as partial sums per CTA
+// (kWgradRows image rows each) that wgrad_reduce_kernel adds up in a fixed order:
+// dw[m][t][k] = sum over pixels p of dz[p][m] * x[p + off(t)][k], db[m] = sum over p of dz[p][m].
+// The GEMM D[(t, k)][m] = sum over p of A[(t, k)][p] * B[m][p] has the 9 CIN (tap, channel) pairs
+// as its rows (M, in tiles of 128), the dz channels as N and the pixels as K.  Per image row
+// (64 pixels) the CTA writes A and B to shared memory in the canonical K-major layout -- each
+// 8 x 8 core matrix is the register transpose of 8 pixels' 16-byte channel vectors -- and one
+// thread issues TILES x 4 MMAs (K = 16) accumulating in TMEM across the CTA's rows.  Row 9 CIN of
+// A is all ones, so D's row 9 CIN is the bias gradient; the remaining padding rows are zero.
+// M = channels of dz as stored (16 or 32), MSTORE = rows of the layer's weight tensor (<= M).
 template <int CIN, int M, int MSTORE>
-__global__ void __launch_bounds__(kWgradThreads) wgrad_kernel(const __nv_bfloat16* __restrict__ x,
-                                                              const __nv_bfloat16* __restrict__ dz,
-                                                              float* __restrict__ part_w,
-                                                              float* __restrict__ part_b) {
-    static_assert(CIN % 16 == 0 && M % 16 == 0 && MSTORE <= M, "channel padding");
-    constexpr int SPX = CIN + 8, SPZ = M + 8;
-    constexpr int HR = kBand + 2, HC = kImg + 2;
-    constexpr int MT = M / 16, NT = CIN / 8;
-    __shared__ __align__(16) __nv_bfloat16 sx[HR * HC * SPX];
-    __shared__ __align__(16) __nv_bfloat16 sz[kBand * kImg * SPZ];
+__global__ void __launch_bounds__(kConvThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                const __nv_bfloat16* __restrict__ dz,
+                                                                float* __restrict__ part_w,
+                                                                float* __restrict__ part_b,
+                                                                unsigned* __restrict__ status) {
+    using L = WgradTcLayout<CIN, M>;
+    static_assert(CIN % 16 == 0 && M % 16 == 0 && MSTORE <= M && L::TILES * M <= 128, "channel padding");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8);
     constexpr int chunks_per_img = kImg / kWgradRows;
     const int img = blockIdx.x / chunks_per_img;
     const int rbase = (blockIdx.x % chunks_per_img) * kWgradRows;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tap = warp, dy = tap / 3, dx = tap % 3;
-    float acc[MT][NT][4];
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0f;
-    float bsum = 0.0f;
-    // ldmatrix row selection: lane i serves row i % 8 of matrix i / 8
-    const int lm = lane >> 3, lr = lane & 7;
-#pragma unroll 1
-    for (int r0 = rbase; r0 < rbase + kWgradRows; r0 += kBand) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < HR * HC * (CIN / 8); i += kWgradThreads) {
-            const int pix = i / (CIN / 8), v = i % (CIN / 8);
-            const int hr = pix / HC, hc = pix % HC;
-            const int gr = r0 + hr - 1, gc = hc - 1;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            if (gr >= 0 && gr < kImg && gc >= 0 && gc < kImg)
-                val = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + v * 8);
-            *reinterpret_cast<uint4*>(sx + pix * SPX + v * 8) = val;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(L::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // rows 9 CIN .. AROWS - 1 of A: the ones row, then zeros; written once
+    {
+        constexpr int first_group = (9 * CIN) / 8, groups = L::AROWS / 8 - first_group;
+        for (int i = tid; i < groups * (L::P / 8) * 8; i += kConvThreads) {
+            const int row = first_group * 8 + (i / ((L::P / 8) * 8)) * 8 + (i % 8);
+            const int pg = (i / 8) % (L::P / 8);
+            const unsigned one = row == 9 * CIN ? 0x3F803F80u : 0u;  // bf16 1.0 pairs
+            *reinterpret_cast<uint4*>(smem + (row >> 3) * L::SBO + pg * 128 + (row & 7) * 16) =
+                make_uint4(one, one, one, one);
         }
-        for (int i = threadIdx.x; i < kBand * kImg * (M / 8); i += kWgradThreads) {
-            const int pix = i / (M / 8), v = i % (M / 8);
-            *reinterpret_cast<uint4*>(sz + pix * SPZ + v * 8) = *reinterpret_cast<const uint4*>(
-                dz + ((int64_t)img * kPix + (int64_t)r0 * kImg + pix) * M + v * 8);
-        }
-        __syncthreads();
-        if (threadIdx.x < M)
-            for (int pix = 0; pix < kBand * kImg; ++pix) bsum += __bfloat162float(sz[pix * SPZ + threadIdx.x]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    constexpr uint32_t idesc = umma_idesc_bf16(128, M);
+    bool ok = true;
+    uint32_t phase = 0;
 #pragma unroll 1
-        for (int k0 = 0; k0 < kBand * kImg; k0 += 16) {
-            // 16 consecutive pixels of one image row
-            const int prow = k0 / kImg, pcol = k0 % kImg;
-            unsigned a[MT][4];
+    for (int row = rbase; row < rbase + kWgradRows && ok; ++row) {
+        // A core matrices: (tap t, channel block kc, pixel group pg) = transpose of the 8 x 8 block
+        // x[pixels 8 pg + j shifted by the tap][channels 8 kc + i] (zero outside the image)
+        for (int i = tid; i < 9 * (CIN / 8) * (L::P / 8); i += kConvThreads) {
+            const int pg = i % (L::P / 8), kc = (i / (L::P / 8)) % (CIN / 8), t = i / ((L::P / 8) * (CIN / 8));
+            const int gr = row + t / 3 - 1;
+            uint4 v[8], o[8];
 #pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                // matrices: (k 0-7, m 0-7), (k 0-7, m 8-15), (k 8-15, m 0-7), (k 8-15, m 8-15)
-                const int kk = k0 + (lm >> 1) * 8 + lr;
-                const int mm = mt * 16 + (lm & 1) * 8;
-                ldsm_x4_trans(a[mt], sz + kk * SPZ + mm);
+            for (int j = 0; j < 8; ++j) {
+                const int gc = 8 * pg + j + t % 3 - 1;
+                v[j] = make_uint4(0u, 0u, 0u, 0u);
+                if (gr >= 0 && gr < kImg && gc >= 0 && gc < kImg)
+                    v[j] = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + kc * 8);
             }
+            transpose8x8_bf16(v, o);
+            const int r0 = t * CIN + kc * 8;
+            uint4* dst = reinterpret_cast<uint4*>(smem + (r0 >> 3) * L::SBO + pg * 128);
 #pragma unroll
-            for (int nt = 0; nt < NT; nt += 2) {
-                // matrices: (k 0-7, n 0-7), (k 8-15, n 0-7), (k 0-7, n 8-15), (k 8-15, n 8-15)
-                const int kc = pcol + (lm & 1) * 8 + lr;
-                const int nn = (nt + (lm >> 1)) * 8;
-                unsigned b[4];
-                ldsm_x4_trans(b, sx + ((prow + dy) * HC + kc + dx) * SPX + nn);
-                const unsigned b0[2] = {b[0], b[1]}, b1[2] = {b[2], b[3]};
+            for (int k = 0; k < 8; ++k) dst[k] = o[k];
+        }
+        // B core matrices: (channel block mc, pixel group pg) = transpose of dz[pixels][channels]
+        for (int i = tid; i < (M / 8) * (L::P / 8); i += kConvThreads) {
+            const int pg = i % (L::P / 8), mc = i / (L::P / 8);
+            uint4 v[8], o[8];
 #pragma unroll
-                for (int mt = 0; mt < MT; ++mt) {
-                    mma_bf16(acc[mt][nt], a[mt], b0);
-                    mma_bf16(acc[mt][nt + 1], a[mt], b1);
+            for (int j = 0; j < 8; ++j)
+                v[j] = *reinterpret_cast<const uint4*>(dz + ((int64_t)(img * kImg + row) * kImg + 8 * pg + j) * M + mc * 8);
+            transpose8x8_bf16(v, o);
+            uint4* dst = reinterpret_cast<uint4*>(smem + L::B_OFF + mc * L::SBO + pg * 128);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) dst[k] = o[k];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            const uint32_t base = smem_u32(smem);
+#pragma unroll 1
+            for (int tile = 0; tile < L::TILES; ++tile)
+#pragma unroll
+                for (int s = 0; s < L::P / 16; ++s) {
+                    const uint32_t a = base + tile * (128 / 8) * L::SBO + 2 * s * 128;
+                    const uint32_t b = base + L::B_OFF + 2 * s * 128;
+                    umma_bf16(tmem + tile * M, umma_desc(a, 128, L::SBO), umma_desc(b, 128, L::SBO), idesc,
+                              (row > rbase || s > 0) ? 1u : 0u);
                 }
+            umma_commit(mbar);
+        }
+        // the operands are rewritten for the next row only after these MMAs have read them
+        bool done = false;
+        for (int it = 0; it < kMmaWaitLimit && !done; ++it) done = mbar_try_wait(mbar, phase);
+        phase ^= 1u;
+        if (!done) {
+            ok = false;
+            if ((tid & 31) == 0) atomicOr(status, kStatusMmaTimeout);
+        }
+        tc_fence_after();
+        __syncthreads();
+    }
+    if (ok) {
+        float* pw = part_w + (int64_t)blockIdx.x * (MSTORE * 9 * CIN);
+#pragma unroll 1
+        for (int tile = 0; tile < L::TILES; ++tile) {
+            const int r = tile * 128 + tid;  // this thread's accumulator row
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + tile * M;
+            float v[32];
+            if constexpr (M == 32) tmem_ld32(taddr, v);
+            else tmem_ld16(taddr, v);
+            if (r < 9 * CIN) {
+                const int t = r / CIN, k = r % CIN;
+#pragma unroll
+                for (int m = 0; m < MSTORE; ++m) pw[(m * 9 + t) * CIN + k] = v[m];
+            } else if (r == 9 * CIN) {
+#pragma unroll
+                for (int m = 0; m < MSTORE; ++m) part_b[(int64_t)blockIdx.x * MSTORE + m] = v[m];
             }
         }
     }
-    const int g = lane >> 2, q = lane & 3;
-    float* pw = part_w + (int64_t)blockIdx.x * (MSTORE * 9 * CIN);
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                const int m = mt * 16 + g + half * 8;
-                const int k = nt * 8 + 2 * q;
-                if (m < MSTORE) {
-                    pw[(m * 9 + tap) * CIN + k] = acc[mt][nt][2 * half];
-                    pw[(m * 9 + tap) * CIN + k + 1] = acc[mt][nt][2 * half + 1];
-                }
-            }
-    if (threadIdx.x < MSTORE) part_b[(int64_t)blockIdx.x * MSTORE + threadIdx.x] = bsum;
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::TMEM_COLS)
+                     : "memory");
+    }
 }
 
 // Sum of the per-CTA partials in CTA order: grad[e] for the weights (nw elements) then the

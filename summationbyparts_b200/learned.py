@@ -311,7 +311,7 @@ def run(pairs: int, heldout: int, epochs: int, fine: int = FINE, lr: float = 2e-
                    "t_end": T_END, "pairs": pairs, "heldout": heldout, "epochs": epochs, "batch": max_batch,
                    "lr": lr, "seed": PAIR_SEED, "restriction": "tensor-product 6-point Lagrange in (xi, eta)",
                    "network": "5 x conv3x3 4-32-32-32-32-4, GELU, bf16 activations, f32 accumulation "
-                              "(tcgen05 convolutions, mma.sync weight gradients)",
+                              "on the tcgen05 tensor cores (convolutions and weight gradients)",
                    "fallback": f"relative size of the network's correction > {fallback_factor} x training maximum"},
         "train": {"loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "seconds": t_train,
                   "data_seconds": t_data, "fine_solve_gpu_seconds": tf_train},
