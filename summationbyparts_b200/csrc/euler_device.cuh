@@ -74,7 +74,13 @@ __device__ __forceinline__ T pressure(T g, T rho, T rhou, T rhov, T e) {
     return (g - T(1)) * (e - (rhou * rhou + rhov * rhov) / (T(2) * rho));
 }
 
-// VortexParameters::evaluate (euler/src/vortex.rs:26-113) at one point, f64.
+// VortexParameters::evaluate (euler/src/vortex.rs:26-113) at one point, f64.  With
+// POW_FREE and gamma == 1.4 the powers are formed from square roots and products: with
+// b = 1 - K e^f, rho = b^(1/(gamma-1)) = b^2.5 = b^2 sqrt(b) and rho^gamma = b^3.5 = b^3 sqrt(b),
+// and e^(f/2) = sqrt(e^f); each is correctly rounded, so the values differ from pow and exp in
+// the last bits only.  The SAT boundary data use that form (it removes the two f64 pow and one
+// exp of every vortex edge point at every stage); initial data and the error norms use pow.
+template <bool POW_FREE = false>
 __device__ inline void vortex_point(const InstanceDev& I, double gamma, double t, double x, double y, double q[4]) {
     const double PI = 3.14159265358979323846;
     const double m = I.mach;
@@ -95,12 +101,22 @@ __device__ inline void vortex_point(const InstanceDev& I, double gamma, double t
         const double dx = (x - I.x0[iv]) - t;
         const double dy = y - I.y0[iv];
         const double f = (1.0 - (dx * dx + dy * dy)) / (rstar * rstar);
-        const double r =
-            pow(1.0 - eps * eps * (gamma - 1.0) * m * m / (8.0 * PI * PI * p_inf * rstar * rstar) * exp(f),
-                1.0 / (gamma - 1.0));
-        const double p = pow(r, gamma) * p_inf;
-        const double u = 1.0 - eps * dy / (2.0 * PI * sqrt(p_inf) * rstar * rstar) * exp(f / 2.0);
-        const double v = eps * dx / (2.0 * PI * sqrt(p_inf) * rstar * rstar) * exp(f / 2.0);
+        double r, p, ef2;
+        if (POW_FREE && gamma == 1.4) {
+            const double ef = exp(f);
+            const double b = 1.0 - eps * eps * (gamma - 1.0) * m * m / (8.0 * PI * PI * p_inf * rstar * rstar) * ef;
+            const double sb = sqrt(b);
+            r = b * b * sb;
+            p = b * b * b * sb * p_inf;
+            ef2 = sqrt(ef);
+        } else {
+            r = pow(1.0 - eps * eps * (gamma - 1.0) * m * m / (8.0 * PI * PI * p_inf * rstar * rstar) * exp(f),
+                    1.0 / (gamma - 1.0));
+            p = pow(r, gamma) * p_inf;
+            ef2 = exp(f / 2.0);
+        }
+        const double u = 1.0 - eps * dy / (2.0 * PI * sqrt(p_inf) * rstar * rstar) * ef2;
+        const double v = eps * dx / (2.0 * PI * sqrt(p_inf) * rstar * rstar) * ef2;
         if (iv == 0) {
             q[0] = r;
             q[1] = r * u;

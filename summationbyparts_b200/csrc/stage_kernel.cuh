@@ -596,7 +596,7 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         const int kind = B.bc_kind[d];
         if (kind == BC_VORTEX) {
             const double* xy = A.xy + B.x_off;
-            vortex_point(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+            vortex_point<true>(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
         } else if (kind == BC_EVAL) {
             // BoundaryCharacteristic::Eval (euler/src/lib.rs:853-863): the expressions at the stage
             // time, evaluated for this edge point by eval_kernel just before
