@@ -17,8 +17,9 @@ namespace cnn {
 
 constexpr int kImg = 64;           // image side: the coarse grid
 constexpr int kPix = kImg * kImg;  // pixels per image
-constexpr int kBand = 2;           // image rows per CTA in the convolution kernels (128 pixels)
-constexpr int kConvThreads = 128;  // 4 warps, 32 pixels each
+constexpr int kBand = 4;           // image rows per CTA of the convolution kernel (256 pixels)
+constexpr int kConvThreads = 256;  // 8 warps: one pixel of the band per thread
+constexpr int kWgradThreads = 128; // 4 warps: one accumulator row of a 128-row tile per thread
 constexpr int kWgradRows = 16;     // image rows per CTA in the weight-gradient kernel
 
 enum Epilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
@@ -132,6 +133,8 @@ template <int CIN, int COUT>
 struct ConvTcLayout {
     static constexpr int NP = COUT < 16 ? 16 : COUT;        // N of the MMA (multiple of 16 for M = 128)
     static constexpr int HR = kBand + 2;                    // halo rows
+    static constexpr int TILES = kBand * kImg / 128;        // M = 128 accumulator tiles (2)
+    static constexpr int TMEM_COLS = TILES * NP <= 32 ? 32 : 64;
     static constexpr int PIX = HR * kImg;                   // pixels of one shifted copy
     static constexpr int CH = CIN / 8;                      // 16-byte channel chunks per pixel
     static constexpr int SBO = CH * 128;                    // bytes between 8-row groups
@@ -149,14 +152,16 @@ __device__ __forceinline__ int canon_off(int row, int kc) {
 
 // 3x3 convolution with zero padding as an implicit GEMM on the tcgen05 tensor cores:
 // out[p][n] = sum over taps t and input channels k of x[p + off(t)][k] * w[n][t][k],
-// off(t) = (t / 3 - 1, t % 3 - 1).  One CTA of 128 threads computes kBand = 2 image rows
-// (M = 128 pixels) for all output channels (N = COUT, at least 16): the input halo goes to
+// off(t) = (t / 3 - 1, t % 3 - 1).  One CTA of 256 threads computes kBand = 4 image rows
+// (two M = 128 pixel tiles, each 2 image rows) for all output channels (N = COUT, at least 16),
+// so the weights are staged once per 256 pixels: the input halo goes to
 // shared memory as three copies shifted by 0, 1 and 2 columns, each in the canonical K-major
 // layout, so the A operand of tap (dy, dx) is copy dx started dy image rows down -- an aligned
-// descriptor offset, no per-tap copy; the weights of the 9 taps follow in the same layout.  One
-// thread issues the 9 * CIN / 16 MMAs (K = 16 each) into a TMEM accumulator of 128 lanes x N
-// f32 columns and commits them to an mbarrier; after the (bounded) wait each warp reads its 32
-// lanes -- one pixel per thread, all channels -- and runs the epilogue:
+// descriptor offset, no per-tap copy (tile h starts 2 h image rows further); the weights of the
+// 9 taps follow in the same layout.  One thread issues the 2 x 9 x CIN / 16 MMAs (K = 16 each)
+// into two TMEM accumulators of 128 lanes x N f32 columns and commits them to an mbarrier; after
+// the (bounded) wait warp w reads lanes 32 (w % 4) .. of tile w / 4 -- one pixel per thread, all
+// channels -- and runs the epilogue:
 //   EPI_GELU   z = acc + bias -> zout (f32), gelu(z) -> yout (bf16)   (hidden layers)
 //   EPI_LINEAR acc + bias -> zout (f32)                                (output layer)
 //   EPI_DGELU  acc * gelu'(zprev) -> yout (bf16)                       (gradient of a hidden layer)
@@ -178,8 +183,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
     const int tid = threadIdx.x, warp = tid >> 5;
 
     if (warp == 0) {
-        // 32 TMEM columns (the allocation minimum) hold the 128 x NP f32 accumulator
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(tslot))
+        // TILES accumulators of 128 lanes x NP f32 columns (32 columns is the allocation minimum)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(L::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -223,9 +229,12 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
             const int dy = t / 3, dx = t % 3;
 #pragma unroll
             for (int j = 0; j < CIN / 16; ++j) {
-                const uint32_t a = base + dx * L::A_BYTES + dy * (kImg / 8) * L::SBO + 2 * j * 128;
                 const uint32_t b = base + L::B_OFF + t * L::B_TAP + 2 * j * 128;
-                umma_bf16(tmem, umma_desc(a, 128, L::SBO), umma_desc(b, 128, L::SBO), idesc, acc);
+#pragma unroll
+                for (int h = 0; h < L::TILES; ++h) {
+                    const uint32_t a = base + dx * L::A_BYTES + (2 * h + dy) * (kImg / 8) * L::SBO + 2 * j * 128;
+                    umma_bf16(tmem + h * L::NP, umma_desc(a, 128, L::SBO), umma_desc(b, 128, L::SBO), idesc, acc);
+                }
                 acc = 1;
             }
         }
@@ -235,9 +244,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
     for (int it = 0; it < kMmaWaitLimit && !done; ++it) done = mbar_try_wait(mbar, 0);
     tc_fence_after();
     if (done) {
-        // thread tid holds accumulator row tid: pixel (r0 + tid / 64, tid % 64)
+        // thread tid holds row tid % 128 of accumulator tid / 128: pixel (r0 + tid / 64, tid % 64)
         const int64_t p = (int64_t)(img * kImg + r0 + tid / kImg) * kImg + tid % kImg;
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (tid / 128) * L::NP;
         float v[32];
         if constexpr (L::NP == 32) tmem_ld32(taddr, v);
         else tmem_ld16(taddr, v);
@@ -262,8 +271,14 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __nv_bfl
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::TMEM_COLS) : "memory");
     }
+}
+
+// Word k (0..3, a compile-time constant after unrolling) of a 16-byte vector, selected without
+// taking the vector's address (which would move it to local memory).
+__device__ __forceinline__ unsigned word_of(const uint4& u, int k) {
+    return k == 0 ? u.x : (k == 1 ? u.y : (k == 2 ? u.z : u.w));
 }
 
 // 8 x 8 transpose of bf16: in[j] holds 8 channels of pixel j, out[i] 8 pixels of channel i.
@@ -273,10 +288,7 @@ __device__ __forceinline__ void transpose8x8_bf16(const uint4 in[8], uint4 out[8
         const unsigned sel = (i & 1) ? 0x7632u : 0x5410u;  // high or low halves of word i / 2
         unsigned w[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const unsigned a = (&in[2 * q].x)[i >> 1], b = (&in[2 * q + 1].x)[i >> 1];
-            w[q] = __byte_perm(a, b, sel);
-        }
+        for (int q = 0; q < 4; ++q) w[q] = __byte_perm(word_of(in[2 * q], i >> 1), word_of(in[2 * q + 1], i >> 1), sel);
         out[i] = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
@@ -307,7 +319,7 @@ struct WgradTcLayout {
 // A is all ones, so D's row 9 CIN is the bias gradient; the remaining padding rows are zero.
 // M = channels of dz as stored (16 or 32), MSTORE = rows of the layer's weight tensor (<= M).
 template <int CIN, int M, int MSTORE>
-__global__ void __launch_bounds__(kConvThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
+__global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
                                                                 const __nv_bfloat16* __restrict__ dz,
                                                                 float* __restrict__ part_w,
                                                                 float* __restrict__ part_b,
@@ -334,7 +346,7 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_tc_kernel(const __nv_bfloa
     // rows 9 CIN .. AROWS - 1 of A: the ones row, then zeros; written once
     {
         constexpr int first_group = (9 * CIN) / 8, groups = L::AROWS / 8 - first_group;
-        for (int i = tid; i < groups * (L::P / 8) * 8; i += kConvThreads) {
+        for (int i = tid; i < groups * (L::P / 8) * 8; i += kWgradThreads) {
             const int row = first_group * 8 + (i / ((L::P / 8) * 8)) * 8 + (i % 8);
             const int pg = (i / 8) % (L::P / 8);
             const unsigned one = row == 9 * CIN ? 0x3F803F80u : 0u;  // bf16 1.0 pairs
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_tc_kernel(const __nv_bfloa
     for (int row = rbase; row < rbase + kWgradRows && ok; ++row) {
         // A core matrices: (tap t, channel block kc, pixel group pg) = transpose of the 8 x 8 block
         // x[pixels 8 pg + j shifted by the tap][channels 8 kc + i] (zero outside the image)
-        for (int i = tid; i < 9 * (CIN / 8) * (L::P / 8); i += kConvThreads) {
+        for (int i = tid; i < 9 * (CIN / 8) * (L::P / 8); i += kWgradThreads) {
             const int pg = i % (L::P / 8), kc = (i / (L::P / 8)) % (CIN / 8), t = i / ((L::P / 8) * (CIN / 8));
             const int gr = row + t / 3 - 1;
             uint4 v[8], o[8];
@@ -371,7 +383,7 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_tc_kernel(const __nv_bfloa
             for (int k = 0; k < 8; ++k) dst[k] = o[k];
         }
         // B core matrices: (channel block mc, pixel group pg) = transpose of dz[pixels][channels]
-        for (int i = tid; i < (M / 8) * (L::P / 8); i += kConvThreads) {
+        for (int i = tid; i < (M / 8) * (L::P / 8); i += kWgradThreads) {
             const int pg = i % (L::P / 8), mc = i / (L::P / 8);
             uint4 v[8], o[8];
 #pragma unroll
