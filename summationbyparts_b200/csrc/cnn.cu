@@ -271,8 +271,8 @@ cudaError_t wgrad(const sbp_cnn* c, int n, int layer, const __nv_bfloat16* x, co
     }
     wgrad_tc_kernel<CIN, M, MSTORE><<<parts, kWgradThreads, bytes, c->st()>>>(x, dz, c->part_w, c->part_b, c->status);
     const int nw = MSTORE * 9 * CIN, nb = MSTORE;
-    wgrad_reduce_kernel<<<(nw + nb + 255) / 256, 256, 0, c->st()>>>(c->part_w, c->part_b, parts, nw, nb,
-                                                                      c->G + c->w_off[layer], c->G + c->b_off[layer]);
+    wgrad_reduce_kernel<<<(nw + nb + 31) / 32, 32 * kReduceSplit, 0, c->st()>>>(
+        c->part_w, c->part_b, parts, nw, nb, c->G + c->w_off[layer], c->G + c->b_off[layer]);
     return cudaGetLastError();
 }
 
