@@ -31,7 +31,8 @@
 // Precision: T = double reproduces the reference's f64 arithmetic operation by operation
 // (compile with -fmad=false).  T = float with COMP = true runs fluxes, dissipation and
 // stencils in f32 and keeps the RK4 state as a (hi, lo) f32 pair; the step's increment
-// sum_j (b_j dt) k_j is accumulated in f32 and added to the pair once per step with TwoSum.
+// sum_j (b_j dt) k_j is accumulated in f32 and added to the pair once per step with TwoSum;
+// the f32 metrics hold 1 / J (rounded from f64), so the flux divergence is scaled by a product.
 // The SAT terms are computed in f64 from f64 metrics.
 #pragma once
 
@@ -107,7 +108,8 @@ struct StageGeom {
 };
 
 // Phase-2 operands staged in shared memory by cp.async while phase 1 runs (compensated-f32
-// kernel): slot 0 detJ, then up to three state arrays x 4 components (see stage_operands).
+// kernel): slot 0 plane 0 of the f32 metrics (1 / J), then up to three state arrays x 4
+// components (see stage_operands).
 constexpr int kStageSlots = 13;
 __host__ __device__ constexpr int staged_elems(bool comp, int TY) { return comp ? kStageSlots * TY * kTileX : 0; }
 
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         const double ca = A.stage < 3 ? I.ca[A.stage] : 0.0;
 
         // ---------------- phase 1: pointwise quantities ----------------
-        // Stage this thread's phase-2 operands (detJ, RK state) into shared memory; the copies
+        // Stage this thread's phase-2 operands (1 / J, RK state) into shared memory; the copies
         // run while phase 1 computes.
         if constexpr (COMP) {
             const int pr0 = y0 + warp * R, prn = min(R, y1 - pr0);
@@ -803,11 +805,12 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
             const bool edge_col = col == 0 || col == nx - 1;
             const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
             const float cbf = float(cb), caf = float(ca);
-            T detj[R];
+            // metrics plane 0: J in f64 (the reference divides by it), 1 / J in the f32 metrics
+            T jac[R];
 #pragma unroll
             for (int u = 0; u < R; ++u) {
-                if constexpr (COMP) detj[u] = u < nrows ? sR[(r0 - y0 + u) * kTileX + lane] : T(1);
-                else detj[u] = u < nrows ? __ldg(mt + (r0 + u) * nx + col) : T(1);
+                if constexpr (COMP) jac[u] = u < nrows ? sR[(r0 - y0 + u) * kTileX + lane] : T(1);
+                else jac[u] = u < nrows ? __ldg(mt + (r0 + u) * nx + col) : T(1);
             }
             T ex[4][R], dx[4][R];
             xi_rows<OPX, DIFF, T, R, !COMP, XA, XP>(sE, r0 - y0, nrows, lx0, col, nx, idxx, xi_closure, A.coef, ex);
@@ -828,8 +831,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
                     if (u < nrows) {
                         const int row = r0 + u;
                         T kc;
-                        if constexpr (UPW) kc = (-ex[cc][u] - dF[u] + dx[cc][u] + ay[u]) / detj[u];
-                        else kc = (-ex[cc][u] - dF[u]) / detj[u];
+                        if constexpr (UPW) kc = -ex[cc][u] - dF[u] + dx[cc][u] + ay[u];
+                        else kc = -ex[cc][u] - dF[u];
+                        if constexpr (COMP) kc = kc * jac[u];
+                        else kc = kc / jac[u];
                         if constexpr (COMP && UPW)
                             kc = kc + I.ref.q[cc] * __ldg(A.rinf + B.r_off + (int64_t)row * nx + col);
                         if (edge_col || row == 0 || row == ny - 1)

@@ -21,7 +21,7 @@
 //   kinds of load are conflict-free.  Tiles that hold closure columns run the table path of
 //   stage_kernel for the xi sums on every thread, so warps do not diverge; for the eta sums
 //   only the threads whose row pair holds a closure row take the table path.
-// * The RK operands (detJ and the stage's state arrays) are read from global memory into
+// * The RK operands (1 / J and the stage's state arrays) are read from global memory into
 //   registers one component ahead of their use, which leaves the shared memory of two
 //   256-thread CTAs per SM to the stencil arrays.
 #pragma once
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                                        sF + (oeta[b] >= 0 ? oeta[b] : 0), YA, oxi[b] >= 0, oeta[b] >= 0, bad);
         }
 
-        // Phase-2 operands of this thread (detJ and component 0's RK operands), loaded before
+        // Phase-2 operands of this thread (1 / J and component 0's RK operands), loaded before
         // the barrier so the loads overlap the other warps' phase 1.  Element of point (u, j)
         // of component cc: in-block offset e0 + cc * np + off[u][j] from the block bases.
         const int c0 = x0 + 2 * grp, r0 = y0 + 2 * rpr;
@@ -266,14 +266,14 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const float* srcb[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) srcb[a] = a < nsrc ? src[a] + qoff : nullptr;
-        float detj[2][2], rinf[2][2], opn[3][2][2];
+        float jinv[2][2], rinf[2][2], opn[3][2][2];  // jinv: plane 0 of the f32 metrics, 1 / J
         const float* rb = UPW ? A.rinf + B.r_off : nullptr;
 #pragma unroll
         for (int u = 0; u < 2; ++u)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const bool ok = rok[u] && cok[j];
-                detj[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
+                jinv[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
                 rinf[u][j] = (UPW && ok) ? __ldg(rb + (e0 + off[u][j])) : 0.0f;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
@@ -365,8 +365,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         const float exv = u == 0 ? ex[j].x : ex[j].y, dxv = u == 0 ? dx[j].x : dx[j].y;
                         const float eyv = j == 0 ? ey[u].x : ey[u].y, ayv = j == 0 ? ay[u].x : ay[u].y;
                         float kc;
-                        if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) / detj[u][j] + qr * rinf[u][j];
-                        else kc = (-exv - eyv) / detj[u][j];
+                        if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) * jinv[u][j] + qr * rinf[u][j];
+                        else kc = (-exv - eyv) * jinv[u][j];
                         const int e = ce + off[u][j];
                         if (edge[u][j]) {
                             const int row = r0 + u, col = c0 + j;

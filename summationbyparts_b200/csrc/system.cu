@@ -1050,7 +1050,10 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         e = e ?: op_apply(D.op_eta, 1, 0, 0, y, tmp + 3 * n, D.ny, D.nx, 1, n, st);
         e = e ?: metrics_combine(tmp, tmp + n, tmp + 2 * n, tmp + 3 * n, n, s->met64 + B.m_off, B.npad, s->status, st);
     }
-    if (e == cudaSuccess && s->met32) e = narrow_f32(s->met64, s->met32, s->nm, st);
+    if (e == cudaSuccess && s->met32) {
+        e = narrow_f32(s->met64, s->met32, s->nm, st);
+        e = e ?: jacobian_inverse_f32(s->d_blocks, nblocks, s->met64, s->met32, s->max_points, st);
+    }
     if (e != cudaSuccess) return fail(cuda_status(e, "metrics"));
     if (s->rinf) {
         // the state starts at zero: in the compensated form a deviation of -qref

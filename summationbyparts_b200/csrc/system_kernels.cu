@@ -295,6 +295,24 @@ cudaError_t narrow_f32(const double* in, float* out, int64_t n, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Plane 0 of each block's single-precision metrics holds 1 / J (rounded once from the f64
+// quotient), so the compensated stage kernels scale the flux divergence by a product.
+__global__ void jacobian_inverse_kernel(const BlockDev* __restrict__ blocks, const double* __restrict__ met64,
+                                        float* __restrict__ met32) {
+    const BlockDev& B = blocks[blockIdx.y];
+    const int64_t n = (int64_t)B.nx * B.ny;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double j = met64[B.m_off + i];
+        met32[B.m_off + i] = j != 0.0 ? float(1.0 / j) : 0.0f;
+    }
+}
+
+cudaError_t jacobian_inverse_f32(const BlockDev* blocks, int nblocks, const double* met64, float* met32,
+                                 int64_t max_points, cudaStream_t st) {
+    jacobian_inverse_kernel<<<per_block_grid(nblocks, max_points), kT, 0, st>>>(blocks, met64, met32);
+    return cudaGetLastError();
+}
+
 cudaError_t vortex_init(const BlockDev* blocks, const InstanceDev* inst, int nblocks, int instance, double gamma,
                         double t, const double* xy, int prec, void* q_hi, void* q_lo, int64_t max_points,
                         cudaStream_t st) {

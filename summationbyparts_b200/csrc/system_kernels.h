@@ -16,6 +16,9 @@ cudaError_t metrics_combine(const double* x_xi, const double* x_eta, const doubl
 
 // Narrow f64 planes to f32 (n elements).
 cudaError_t narrow_f32(const double* in, float* out, int64_t n, cudaStream_t st);
+// Plane 0 (J) of every block's f32 metrics replaced by 1 / J, rounded from the f64 quotient.
+cudaError_t jacobian_inverse_f32(const BlockDev* blocks, int nblocks, const double* met64, float* met32,
+                                 int64_t max_points, cudaStream_t st);
 
 // Vortex initial data for every block whose instance is selected (instance < 0: all).
 // f64 state: q_hi only.  f32 state: (hi, lo) split of the f64 value.
