@@ -20,7 +20,7 @@ constexpr int kPix = kImg * kImg;  // pixels per image
 constexpr int kBand = 4;           // image rows per CTA of the convolution kernel (256 pixels)
 constexpr int kConvThreads = 256;  // 8 warps: one pixel of the band per thread
 constexpr int kWgradThreads = 128; // 4 warps: one accumulator row of a 128-row tile per thread
-constexpr int kWgradRows = 8;      // image rows per CTA in the weight-gradient kernel
+constexpr int kWgradRows = 4;      // image rows per CTA in the weight-gradient kernel
 
 enum Epilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
 
@@ -313,7 +313,11 @@ __device__ __forceinline__ void transpose8x8_bf16(const uint4 in[8], uint4 out[8
     }
 }
 
-// Shared-memory layout of the tcgen05 weight-gradient kernel.
+// Shared-memory layout of the tcgen05 weight-gradient kernel: the canonical A and B operands of
+// one image row, then the CTA's raw input rows (x with one halo row on each side, dz) as copied
+// from global memory.  Raw rows hold pixels channel-innermost with 16 bytes of padding after every
+// 8 pixels, so 8 threads reading the same channel chunk of 8 consecutive pixel groups hit 8
+// different 16-byte bank groups.
 template <int CIN, int M>
 struct WgradTcLayout {
     static constexpr int ROWS = 9 * CIN + 1;                // (tap, input channel) rows + the ones row
@@ -323,20 +327,32 @@ struct WgradTcLayout {
     static constexpr int SBO = (P / 8) * 128;               // bytes between 8-row groups
     static constexpr int A_BYTES = AROWS * P * 2;
     static constexpr int B_OFF = A_BYTES;
-    static constexpr int BAR_OFF = B_OFF + M * P * 2;
+    static constexpr int XROW = P * CIN * 2 + (P / 8) * 16;  // bytes of one raw x row
+    static constexpr int ZROW = P * M * 2 + (P / 8) * 16;    // bytes of one raw dz row
+    static constexpr int XR_OFF = B_OFF + M * P * 2;
+    static constexpr int ZR_OFF = XR_OFF + (kWgradRows + 2) * XROW;
+    static constexpr int BAR_OFF = ZR_OFF + kWgradRows * ZROW;
     static constexpr int BYTES = BAR_OFF + 16;
     static constexpr int TMEM_COLS = TILES * M <= 32 ? 32 : (TILES * M <= 64 ? 64 : 128);
 };
+
+// Byte offset of pixel c, channel chunk kc of a raw row (C channels per pixel).
+template <int C>
+__device__ __forceinline__ int raw_off(int c, int kc) {
+    return c * C * 2 + (c >> 3) * 16 + kc * 16;
+}
 
 // Weight and bias gradients of one layer on the tcgen05 tensor cores, as partial sums per CTA
 // (kWgradRows image rows each) that wgrad_reduce_kernel adds up in a fixed order:
 // dw[m][t][k] = sum over pixels p of dz[p][m] * x[p + off(t)][k], db[m] = sum over p of dz[p][m].
 // The GEMM D[(t, k)][m] = sum over p of A[(t, k)][p] * B[m][p] has the 9 CIN (tap, channel) pairs
-// as its rows (M, in tiles of 128), the dz channels as N and the pixels as K.  Per image row
-// (64 pixels) the CTA writes A and B to shared memory in the canonical K-major layout -- each
-// 8 x 8 core matrix is the register transpose of 8 pixels' 16-byte channel vectors -- and one
-// thread issues TILES x 4 MMAs (K = 16) accumulating in TMEM across the CTA's rows.  Row 9 CIN of
-// A is all ones, so D's row 9 CIN is the bias gradient; the remaining padding rows are zero.
+// as its rows (M, in tiles of 128), the dz channels as N and the pixels as K.  The CTA's raw rows
+// of x (with the halo rows, zero outside the image) and dz arrive first, by 16-byte asynchronous
+// copies all in flight at once.  Per image row (64 pixels) the threads then write A and B in the
+// canonical K-major layout -- each 8 x 8 core matrix the register transpose of 8 pixels' 16-byte
+// channel vectors read from the raw rows -- and one thread issues TILES x 4 MMAs (K = 16)
+// accumulating in TMEM across the CTA's rows.  Row 9 CIN of A is all ones, so D's row 9 CIN is
+// the bias gradient; the remaining padding rows are zero.
 // M = channels of dz as stored (16 or 32), MSTORE = rows of the layer's weight tensor (<= M).
 template <int CIN, int M, int MSTORE>
 __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
@@ -346,6 +362,7 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
                                                                 unsigned* __restrict__ status) {
     using L = WgradTcLayout<CIN, M>;
     static_assert(CIN % 16 == 0 && M % 16 == 0 && MSTORE <= M && L::TILES * M <= 128, "channel padding");
+    constexpr int XCH = CIN / 8, ZCH = M / 8;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + L::BAR_OFF + 8);
@@ -353,6 +370,20 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
     const int img = blockIdx.x / chunks_per_img;
     const int rbase = (blockIdx.x % chunks_per_img) * kWgradRows;
     const int tid = threadIdx.x, warp = tid >> 5;
+    // raw rows: x rows rbase - 1 .. rbase + kWgradRows (zero-filled outside the image), dz rows
+    // rbase .. rbase + kWgradRows - 1
+    for (int i = tid; i < (kWgradRows + 2) * L::P * XCH; i += kWgradThreads) {
+        const int kc = i % XCH, c = (i / XCH) % L::P, hr = i / (XCH * L::P);
+        const int gr = rbase + hr - 1;
+        const bool in = gr >= 0 && gr < kImg;
+        cp_async16(smem + L::XR_OFF + hr * L::XROW + raw_off<CIN>(c, kc),
+                   x + ((int64_t)(img * kImg + (in ? gr : 0)) * kImg + c) * CIN + kc * 8, in ? 16u : 0u);
+    }
+    for (int i = tid; i < kWgradRows * L::P * ZCH; i += kWgradThreads) {
+        const int kc = i % ZCH, c = (i / ZCH) % L::P, hr = i / (ZCH * L::P);
+        cp_async16(smem + L::ZR_OFF + hr * L::ZROW + raw_off<M>(c, kc),
+                   dz + ((int64_t)(img * kImg + rbase + hr) * kImg + c) * M + kc * 8, 16u);
+    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(L::TMEM_COLS)
@@ -374,6 +405,7 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
                 make_uint4(one, one, one, one);
         }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -382,19 +414,20 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
     bool ok = true;
     uint32_t phase = 0;
 #pragma unroll 1
-    for (int row = rbase; row < rbase + kWgradRows && ok; ++row) {
+    for (int lr = 0; lr < kWgradRows && ok; ++lr) {
         // A core matrices: (tap t, channel block kc, pixel group pg) = transpose of the 8 x 8 block
-        // x[pixels 8 pg + j shifted by the tap][channels 8 kc + i] (zero outside the image)
-        for (int i = tid; i < 9 * (CIN / 8) * (L::P / 8); i += kWgradThreads) {
-            const int pg = i % (L::P / 8), kc = (i / (L::P / 8)) % (CIN / 8), t = i / ((L::P / 8) * (CIN / 8));
-            const int gr = row + t / 3 - 1;
+        // x[pixels 8 pg + j shifted by the tap][channels 8 kc + i] (zero outside the image).
+        // Consecutive threads take consecutive pixel groups: conflict-free raw reads (padding) and
+        // canonical writes (128 bytes apart).
+        for (int i = tid; i < 9 * XCH * (L::P / 8); i += kWgradThreads) {
+            const int pg = i % (L::P / 8), kc = (i / (L::P / 8)) % XCH, t = i / ((L::P / 8) * XCH);
+            const unsigned char* src = smem + L::XR_OFF + (lr + t / 3) * L::XROW;
             uint4 v[8], o[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int gc = 8 * pg + j + t % 3 - 1;
-                v[j] = make_uint4(0u, 0u, 0u, 0u);
-                if (gr >= 0 && gr < kImg && gc >= 0 && gc < kImg)
-                    v[j] = *reinterpret_cast<const uint4*>(x + ((int64_t)(img * kImg + gr) * kImg + gc) * CIN + kc * 8);
+                v[j] = (gc >= 0 && gc < kImg) ? *reinterpret_cast<const uint4*>(src + raw_off<CIN>(gc, kc))
+                                              : make_uint4(0u, 0u, 0u, 0u);
             }
             transpose8x8_bf16(v, o);
             const int r0 = t * CIN + kc * 8;
@@ -403,12 +436,12 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
             for (int k = 0; k < 8; ++k) dst[k] = o[k];
         }
         // B core matrices: (channel block mc, pixel group pg) = transpose of dz[pixels][channels]
-        for (int i = tid; i < (M / 8) * (L::P / 8); i += kWgradThreads) {
+        for (int i = tid; i < ZCH * (L::P / 8); i += kWgradThreads) {
             const int pg = i % (L::P / 8), mc = i / (L::P / 8);
+            const unsigned char* src = smem + L::ZR_OFF + lr * L::ZROW;
             uint4 v[8], o[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                v[j] = *reinterpret_cast<const uint4*>(dz + ((int64_t)(img * kImg + row) * kImg + 8 * pg + j) * M + mc * 8);
+            for (int j = 0; j < 8; ++j) v[j] = *reinterpret_cast<const uint4*>(src + raw_off<M>(8 * pg + j, mc));
             transpose8x8_bf16(v, o);
             uint4* dst = reinterpret_cast<uint4*>(smem + L::B_OFF + mc * L::SBO + pg * 128);
 #pragma unroll
@@ -427,7 +460,7 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
                     const uint32_t a = base + tile * (128 / 8) * L::SBO + 2 * s * 128;
                     const uint32_t b = base + L::B_OFF + 2 * s * 128;
                     umma_bf16(tmem + tile * M, umma_desc(a, 128, L::SBO), umma_desc(b, 128, L::SBO), idesc,
-                              (row > rbase || s > 0) ? 1u : 0u);
+                              (lr > 0 || s > 0) ? 1u : 0u);
                 }
             umma_commit(mbar);
         }
@@ -474,7 +507,7 @@ __global__ void __launch_bounds__(kWgradThreads) wgrad_tc_kernel(const __nv_bflo
 // biases (nb elements).  A CTA of 32 x kReduceSplit threads covers 32 elements: thread (lane, g)
 // sums the partials g, g + kReduceSplit, ... of element lane in that order (coalesced across
 // lanes), and lane's kReduceSplit sums are then added in order of g.
-constexpr int kReduceSplit = 8;
+constexpr int kReduceSplit = 32;
 __global__ void __launch_bounds__(32 * kReduceSplit) wgrad_reduce_kernel(const float* __restrict__ part_w,
                                                                        const float* __restrict__ part_b, int nparts,
                                                                        int nw, int nb, float* __restrict__ gw,
