@@ -10,9 +10,9 @@ namespace sbp {
     if (opx == OX && opy == OY && upw == UPW && ty == 16 && TYV == 16)                \
         return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, 16>); \
     if (opx == OX && opy == OY && upw == UPW && ty == kVecRows && TYV == kVecRows)    \
-        return reinterpret_cast<const void*>(&stage_kernel_vec<OX, OY, UPW>);
+        return vec_entry<OX, OY, UPW>(sc);
 
-const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f32_sbp(int opx, int opy, bool upw, int ty, int sc) {
     CASE(SBP4, SBP4, false, 16)
     CASE(SBP4, SBP4, false, 32)
     CASE(SBP8, SBP8, false, 16)

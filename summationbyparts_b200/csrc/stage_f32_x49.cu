@@ -12,10 +12,10 @@ namespace sbp {
 #define CASE(OX, OY, UPW)                                                                          \
     if (opx == OX && opy == OY && upw == UPW) {                                                     \
         if (ty == 16) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, float, UPW, true, 16>); \
-        if (ty == kVecRows) return reinterpret_cast<const void*>(&stage_kernel_vec<OX, OY, UPW>);   \
+        if (ty == kVecRows) return vec_entry<OX, OY, UPW>(sc);   \
     }
 
-const void* stage_ptr_f32_x49(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f32_x49(int opx, int opy, bool upw, int ty, int sc) {
     CASE(UPWIND4, UPWIND9, true)
     CASE(UPWIND4, UPWIND9, false)
     CASE(UPWIND4, UPWIND9H2, true)

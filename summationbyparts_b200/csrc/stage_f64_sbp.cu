@@ -8,7 +8,8 @@ namespace sbp {
     if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
         return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, TYV>);
 
-const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f64_sbp(int opx, int opy, bool upw, int ty, int sc) {
+    (void)sc;  // the f64 kernels take the stage at run time
     CASE(SBP4, SBP4, false, 16)
     CASE(SBP4, SBP4, false, 32)
     CASE(SBP8, SBP8, false, 16)

@@ -8,7 +8,8 @@ namespace sbp {
     if (opx == OX && opy == OY && upw == UPW && ty == TYV)        \
         return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, TYV>);
 
-const void* stage_ptr_f64_u9(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f64_u9(int opx, int opy, bool upw, int ty, int sc) {
+    (void)sc;  // the f64 kernels take the stage at run time
     CASE(UPWIND9, UPWIND9, true, 16)
     CASE(UPWIND9, UPWIND9, true, 32)
     CASE(UPWIND9, UPWIND9, false, 16)

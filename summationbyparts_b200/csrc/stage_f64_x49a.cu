@@ -13,7 +13,8 @@ namespace sbp {
         if (ty == 32) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 32>); \
     }
 
-const void* stage_ptr_f64_x49a(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f64_x49a(int opx, int opy, bool upw, int ty, int sc) {
+    (void)sc;  // the f64 kernels take the stage at run time
     CASE(UPWIND4, UPWIND9, true)
     CASE(UPWIND4, UPWIND9, false)
     CASE(UPWIND4, UPWIND9H2, true)

@@ -13,7 +13,8 @@ namespace sbp {
         if (ty == 32) return reinterpret_cast<const void*>(&stage_kernel<OX, OY, double, UPW, false, 32>); \
     }
 
-const void* stage_ptr_f64_x49b(int opx, int opy, bool upw, int ty) {
+const void* stage_ptr_f64_x49b(int opx, int opy, bool upw, int ty, int sc) {
+    (void)sc;  // the f64 kernels take the stage at run time
     CASE(UPWIND9, UPWIND4, true)
     CASE(UPWIND9, UPWIND4, false)
     CASE(UPWIND9, UPWIND4H2, true)

@@ -157,8 +157,14 @@ constexpr size_t vec_stage_smem(bool upw) {
     return sizeof(float) * (size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1);
 }
 
-template <int OPX, int OPY, bool UPW>
+// Stage class of the RK update: 0 = stage 0, 1 = stages 1 and 2, 2 = stage 3.  The micro-tile
+// kernel takes it as a template parameter, so the operand arrays it reads and the update it
+// writes are fixed at compile time (the k-only stage of other tableaus runs on f64 systems only).
+__host__ __device__ constexpr int vec_stage_class(int stage) { return stage == 0 ? 0 : (stage < 3 ? 1 : 2); }
+
+template <int OPX, int OPY, bool UPW, int SC>
 __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const StageArgs<float> A) {
+    static_assert(SC >= 0 && SC <= 2, "stage class");
     using G = VecGeom<OPX, OPY>;
     constexpr int TY = kVecRows;
     constexpr int XA = G::XA, YA = G::YA, XCH = G::XCH;
@@ -173,8 +179,13 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     const int tid = threadIdx.x;
     const int grp = tid & 15, rpr = tid >> 4;  // column pair, row pair (0..15 each)
     unsigned bad = 0;
-    const float* src[3] = {nullptr, nullptr, nullptr};
-    const int nsrc = A.stage == kStageK ? 0 : stage_operands<float>(A, src);
+    if (A.stage == kStageK || vec_stage_class(A.stage) != SC) {  // launched for another stage class
+        if (tid == 0) atomicOr(A.status, STATUS_BAD_LAUNCH);
+        return;
+    }
+    // RK operand arrays (stage_operands): stage 0 u_in; stages 1, 2 acc_hi, prev_hi; stage 3 also prev_lo
+    constexpr int NSRC = SC + 1;
+    const float* src[3] = {SC == 0 ? A.u_in : A.acc_hi, A.prev_hi, A.prev_lo};
 
     for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
         const int4 td = A.tiles[t];
@@ -265,7 +276,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const int off[2][2] = {{0, 1}, {nx, nx + 1}};
         const float* srcb[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) srcb[a] = a < nsrc ? src[a] + qoff : nullptr;
+        for (int a = 0; a < 3; ++a) srcb[a] = a < NSRC ? src[a] + qoff : nullptr;
         float jinv[2][2], rinf[2][2], opn[3][2][2];  // jinv: plane 0 of the f32 metrics, 1 / J
         const float* rb = UPW ? A.rinf + B.r_off : nullptr;
 #pragma unroll
@@ -276,7 +287,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 jinv[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
                 rinf[u][j] = (UPW && ok) ? __ldg(rb + (e0 + off[u][j])) : 0.0f;
 #pragma unroll
-                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < nsrc) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
+                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < NSRC) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
             }
         __syncthreads();
 
@@ -317,8 +328,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 el[u].to = 0;
             }
             // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
-            float* out1 = (A.stage == 3 ? A.new_hi : A.u_out) + qoff;
-            float* out2 = (A.stage == 3 ? A.new_lo : A.acc_hi) + qoff;
+            float* out1 = (SC == 2 ? A.new_hi : A.u_out) + qoff;
+            float* out2 = (SC == 2 ? A.new_lo : A.acc_hi) + qoff;
 #pragma unroll 1
             for (int cc = 0; cc < 4; ++cc) {
                 const int ce = e0 + cc * np;
@@ -331,7 +342,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         for (int j = 0; j < 2; ++j)
 #pragma unroll
                             for (int a = 0; a < 3; ++a)
-                                nxt[a][u][j] = (rok[u] && cok[j] && a < nsrc) ? __ldg(srcb[a] + (ce + np + off[u][j])) : 0.0f;
+                                nxt[a][u][j] = (rok[u] && cok[j] && a < NSRC) ? __ldg(srcb[a] + (ce + np + off[u][j])) : 0.0f;
                 }
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
@@ -371,12 +382,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         if (edge[u][j]) {
                             const int row = r0 + u, col = c0 + j;
                             A.kedge[4 * (eoff + edge_index(row, col, nx, ny)) + cc] = kc;
-                        } else if (A.stage == kStageK) {
-                            out1[e] = kc;
-                        } else if (A.stage == 0) {
+                        } else if constexpr (SC == 0) {
                             out1[e] = opn[0][u][j] + caf * kc;
                             out2[e] = cbf * kc;
-                        } else if (A.stage < 3) {
+                        } else if constexpr (SC == 1) {
                             out1[e] = opn[1][u][j] + caf * kc;
                             out2[e] = opn[0][u][j] + cbf * kc;
                         } else {
@@ -388,7 +397,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     }
                 if (cc < 3) {
 #pragma unroll
-                    for (int a = 0; a < 3; ++a)
+                    for (int a = 0; a < NSRC; ++a)
 #pragma unroll
                         for (int u = 0; u < 2; ++u)
 #pragma unroll
@@ -400,6 +409,14 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         __syncthreads();
     }
     if (bad) atomicOr(A.status, bad);
+}
+
+// Entry of the micro-tile kernel for stage class sc (vec_stage_class), for cudaLaunchKernel.
+template <int OPX, int OPY, bool UPW>
+const void* vec_entry(int sc) {
+    if (sc == 0) return reinterpret_cast<const void*>(&stage_kernel_vec<OPX, OPY, UPW, 0>);
+    if (sc == 1) return reinterpret_cast<const void*>(&stage_kernel_vec<OPX, OPY, UPW, 1>);
+    return reinterpret_cast<const void*>(&stage_kernel_vec<OPX, OPY, UPW, 2>);
 }
 
 }  // namespace sbp

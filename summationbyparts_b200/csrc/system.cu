@@ -29,8 +29,8 @@ namespace sbp {
 const double* op_h_weights(int op);
 void fill_coef_table(int prec, void* out, int stride, int row);
 
-const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty) {
-    using F = const void* (*)(int, int, bool, int);
+const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty, int sc) {
+    using F = const void* (*)(int, int, bool, int, int);
     static const F f64[] = {stage_ptr_f64_u4,   stage_ptr_f64_u9,   stage_ptr_f64_sbp, stage_ptr_f64_x49a,
                             stage_ptr_f64_x49b, stage_ptr_f64_xsa, stage_ptr_f64_xsb};
     static const F f32[] = {stage_ptr_f32_u4, stage_ptr_f32_u9, stage_ptr_f32_sbp, stage_ptr_f32_x49,
@@ -38,7 +38,7 @@ const void* stage_kernel_ptr(int prec, int opx, int opy, bool upw, int ty) {
     const F* fs = prec == 0 ? f64 : f32;
     const size_t nf = prec == 0 ? sizeof(f64) / sizeof(F) : sizeof(f32) / sizeof(F);
     for (size_t i = 0; i < nf; ++i) {
-        const void* p = fs[i](opx, opy, upw, ty);
+        const void* p = fs[i](opx, opy, upw, ty, sc);
         if (p) return p;
     }
     return nullptr;
@@ -86,7 +86,8 @@ size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
 struct Group {
     int opx, opy;
     bool upw;
-    const void* fn;
+    const void* fn[3];  // stage kernel per RK stage class (vec_stage_class); the same entry thrice
+                        // for kernels that take the stage at run time
     int4* d_tiles = nullptr;
     int ntiles = 0;
     int4* d_edges = nullptr;  // (block, row, col) of every edge point of the group's blocks
@@ -352,7 +353,7 @@ sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t s
     if (s->prec == 0) {
         StageArgs<double> a = stage_args<double>(s, stage, g);
         void* args[] = {&a};
-        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        e = cudaLaunchKernel(g.fn[vec_stage_class(stage)], dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
         if (e == cudaSuccess && edges_too && s->has_eval)
             e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
@@ -360,7 +361,7 @@ sbp_status launch_group(sbp_system* s, int stage, const Group& g, cudaStream_t s
     } else {
         StageArgs<float> a = stage_args<float>(s, stage, g);
         void* args[] = {&a};
-        e = cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st);
+        e = cudaLaunchKernel(g.fn[vec_stage_class(stage)], dim3(g.grid), dim3(s->threads), args, g.smem, st);
         void* sargs[] = {&a, &edges, &nedges};
         if (e == cudaSuccess && edges_too && s->has_eval)
             e = cudaLaunchKernel(evk, sat_grid, dim3(kSatThreads), sargs, 0, st);
@@ -492,8 +493,8 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
                     g.ty = c.ty;
                     g.ctas = c.ctas;
                 }
-            g.fn = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw, g.ty);
-            if (!g.fn) {
+            for (int sc = 0; sc < 3; ++sc) g.fn[sc] = stage_kernel_ptr(s->prec, B.op_xi, B.op_eta, upw, g.ty, sc);
+            if (!g.fn[0] || !g.fn[1] || !g.fn[2]) {
                 set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", B.op_xi, B.op_eta);
                 return SBP_ERR_UNSUPPORTED;
             }
@@ -550,9 +551,13 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             set_error("tile %dx%d needs %zu bytes of shared memory (limit %zu)", TY, TX, g.smem, s->smem_optin);
             return SBP_ERR_INVALID_ARGUMENT;
         }
-        SBP_TRY_CUDA(cudaFuncSetAttribute(g.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
-        int per_sm = 0;
-        SBP_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g.fn, s->threads, g.smem));
+        int per_sm = 1 << 30;
+        for (int sc = 0; sc < 3; ++sc) {
+            SBP_TRY_CUDA(cudaFuncSetAttribute(g.fn[sc], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+            int n = 0;
+            SBP_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, g.fn[sc], s->threads, g.smem));
+            per_sm = std::min(per_sm, n);
+        }
         if (per_sm < 1) {
             set_error("stage kernel cannot be resident with %d threads and %zu bytes shared memory", s->threads,
                       g.smem);
@@ -628,6 +633,10 @@ sbp_status check_status(sbp_system* s) {
     unsigned hs = 0;
     SBP_TRY_CUDA(cudaMemcpyAsync(&hs, s->status, sizeof hs, cudaMemcpyDeviceToHost, s->st()));
     SBP_TRY_CUDA(cudaStreamSynchronize(s->st()));
+    if (hs & STATUS_BAD_LAUNCH) {
+        set_error("internal: a stage kernel was launched for another RK stage class (flags 0x%x)", hs);
+        return SBP_ERR_INVALID_ARGUMENT;
+    }
     if (hs) {
         set_error("non-physical state detected on device (flags 0x%x: 1 rho<=0, 2 p<=0, 4 detJ<=0)", hs);
         return SBP_ERR_NONPHYSICAL;
@@ -666,7 +675,7 @@ sbp_status launch_rhs(sbp_system* s, const double* u_in, double* k_out, double c
         a.u_in = u_in;
         a.u_out = k_out;
         void* args[] = {&a};
-        SBP_TRY_CUDA(cudaLaunchKernel(g.fn, dim3(g.grid), dim3(s->threads), args, g.smem, st));
+        SBP_TRY_CUDA(cudaLaunchKernel(g.fn[0], dim3(g.grid), dim3(s->threads), args, g.smem, st));  // f64: one entry
         int4* edges = g.d_edges;
         int nedges = g.nedges;
         void* sargs[] = {&a, &edges, &nedges};
@@ -1074,7 +1083,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
         OpInfo ox, oy;
         op_info(s->hb[b].op_xi, ox);
         op_info(s->hb[b].op_eta, oy);
-        if (!stage_kernel_ptr(s->prec, s->hb[b].op_xi, s->hb[b].op_eta, ox.upwind && oy.upwind, 16)) {
+        if (!stage_kernel_ptr(s->prec, s->hb[b].op_xi, s->hb[b].op_eta, ox.upwind && oy.upwind, 16, 0)) {
             set_error("operator pair (xi %d, eta %d) is not built into the stage kernels", s->hb[b].op_xi,
                       s->hb[b].op_eta);
             return fail(SBP_ERR_UNSUPPORTED);
