@@ -93,6 +93,29 @@ SBP_COEF_ALL_DISS(UPWIND9H2, UPWIND9H2)
 #undef SBP_COEF_ALL
 #undef SBP_COEF_ALL_DISS
 
+
+// The interior diagonals in f32 as compile-time constants (the same literals as the constant
+// tables): the paired-FMA stencils of the micro-tile kernel take their coefficients from here, so
+// each tap's coefficient is an immediate and the zero tap of a central difference is skipped.
+template <int OP, int KIND>
+struct CDiag;
+#define SBP_CD(OP, TAG, KINDV, KINDN)                                           \
+    template <>                                                                  \
+    struct CDiag<OP, KINDV> {                                                    \
+        static constexpr float v[] = {SBPC_##TAG##_##KINDN##_DIAG(SBPC_LIT_F32)}; \
+    };
+SBP_CD(UPWIND4, UPWIND4, DIFF, DIFF)
+SBP_CD(UPWIND4H2, UPWIND4H2, DIFF, DIFF)
+SBP_CD(UPWIND9, UPWIND9, DIFF, DIFF)
+SBP_CD(UPWIND9H2, UPWIND9H2, DIFF, DIFF)
+SBP_CD(SBP4, SBP4, DIFF, DIFF)
+SBP_CD(SBP8, SBP8, DIFF, DIFF)
+SBP_CD(UPWIND4, UPWIND4, DISS, DISS)
+SBP_CD(UPWIND4H2, UPWIND4H2, DISS, DISS)
+SBP_CD(UPWIND9, UPWIND9, DISS, DISS)
+SBP_CD(UPWIND9H2, UPWIND9H2, DISS, DISS)
+#undef SBP_CD
+
 template <int OP, int KIND, class T>
 __device__ __forceinline__ T coef_end(int i, int k) {
     constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N;

@@ -49,22 +49,40 @@ __device__ __forceinline__ int xslot(int c) { return (c >> 1) + (c & 1) * XCH; }
 __device__ __forceinline__ float2 ffma2(float2 a, float c, float2 acc) { return __ffma2_rn(a, make_float2(c, c), acc); }
 __device__ __forceinline__ float2 fmul2s(float2 a, float c) { return __fmul2_rn(a, make_float2(c, c)); }
 
+// Taps I..D of two adjacent outputs of one stencil: ld(i) is the input pair at tap position i of
+// the first output (D + 1 positions for the two); output 0 takes coefficient i at position i,
+// output 1 coefficient i - 1.  Unrolled at compile time so every coefficient is a constant and
+// zero coefficients cost nothing.
+template <int OP, int KIND, int I, int D>
+struct PairTaps {
+    template <class LD>
+    __device__ __forceinline__ static void run(const LD& ld, float2& a0, float2& a1) {
+        if constexpr (I <= D) {
+            const float2 v = ld(I);
+            if constexpr (I < D) {
+                constexpr float c = CDiag<OP, KIND>::v[I];
+                if constexpr (c != 0.0f) a0 = ffma2(v, c, a0);
+            }
+            if constexpr (I >= 1) {
+                constexpr float c = CDiag<OP, KIND>::v[I - 1];
+                if constexpr (c != 0.0f) a1 = ffma2(v, c, a1);
+            }
+            PairTaps<OP, KIND, I + 1, D>::run(ld, a0, a1);
+        }
+    }
+};
+
 // Xi sums of one kind at columns c0, c0 + 1, each over the thread's two rows.  Local column
 // c0 - H + i of the transposed array, row r0, is at (i even ? pe : po) + (i / 2) * kVecPitch
 // (pe, po: the slots of columns c0 - H and c0 - H + 1; 8-byte aligned).  Interior columns: the
-// fma chain of stage_kernel's interior path.
+// fma chain of stage_kernel's interior path (its zero taps skipped).
 template <int OP, int KIND>
 __device__ __forceinline__ void xi_pair(const float* __restrict__ pe, const float* __restrict__ po, float idx,
                                         float2 out[2]) {
     constexpr int D = OpShape<OP>::D;
-    using C = Coef<OP, KIND, float>;
     float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
-#pragma unroll
-    for (int i = 0; i <= D; ++i) {
-        const float2 v = *reinterpret_cast<const float2*>((i & 1 ? po : pe) + (i >> 1) * kVecPitch);
-        if (i < D) a0 = ffma2(v, C::diag(i), a0);
-        if (i >= 1) a1 = ffma2(v, C::diag(i - 1), a1);
-    }
+    PairTaps<OP, KIND, 0, D>::run(
+        [&](int i) { return *reinterpret_cast<const float2*>((i & 1 ? po : pe) + (i >> 1) * kVecPitch); }, a0, a1);
     out[0] = fmul2s(a0, idx);
     out[1] = fmul2s(a1, idx);
 }
@@ -74,14 +92,8 @@ __device__ __forceinline__ void xi_pair(const float* __restrict__ pe, const floa
 template <int OP, int KIND>
 __device__ __forceinline__ void eta_pair(const float* __restrict__ p, float idx, float2 out[2]) {
     constexpr int D = OpShape<OP>::D;
-    using C = Coef<OP, KIND, float>;
     float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
-#pragma unroll
-    for (int i = 0; i <= D; ++i) {
-        const float2 v = *reinterpret_cast<const float2*>(p + i * kTileX);
-        if (i < D) a0 = ffma2(v, C::diag(i), a0);
-        if (i >= 1) a1 = ffma2(v, C::diag(i - 1), a1);
-    }
+    PairTaps<OP, KIND, 0, D>::run([&](int i) { return *reinterpret_cast<const float2*>(p + i * kTileX); }, a0, a1);
     out[0] = fmul2s(a0, idx);
     out[1] = fmul2s(a1, idx);
 }
@@ -169,6 +181,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     constexpr int TY = kVecRows;
     constexpr int XA = G::XA, YA = G::YA, XCH = G::XCH;
     constexpr int HX = OpShape<OPX>::H, HY = OpShape<OPY>::H;
+    // phase-1 points per thread and batch: enough for an interior tile's whole region
+    // ((32 + 2 H_eta) rows x 32 + 32 rows x 2 H_xi points) in one batch of loads
     // phase-1 points per thread and batch: enough for an interior tile's whole region
     // ((32 + 2 H_eta) rows x 32 + 32 rows x 2 H_xi points) in one batch of loads
     constexpr int P1B = ((kVecRows + 2 * HY) * kTileX + kVecRows * 2 * HX + kStageThreads - 1) / kStageThreads;
@@ -311,6 +325,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
             // table-path descriptors of the thread's columns (xi closure tiles) and rows (eta closure
             // tiles); an output past the tile repeats the first one
             TableLine xl[2], el[2];
+            if (xi_closure) {
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 int trow, base;
@@ -319,6 +334,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 xl[j].te = xslot<XCH>(base - lx0) * kVecPitch;
                 xl[j].to = xslot<XCH>(base - lx0 + 1) * kVecPitch;
             }
+            }
+            if (eta_closure) {
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 int trow, base;
@@ -327,12 +344,18 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 el[u].te = (base - ly0) * kTileX;
                 el[u].to = 0;
             }
+            }
             // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
-            float* out1 = (SC == 2 ? A.new_hi : A.u_out) + qoff;
-            float* out2 = (SC == 2 ? A.new_lo : A.acc_hi) + qoff;
+            // per-array pointers at point (r0, c0) of component cc, advanced by one plane per
+            // component: the four points are at offsets 0, 1, nx, nx + 1
+            float* out1 = (SC == 2 ? A.new_hi : A.u_out) + qoff + e0;
+            float* out2 = (SC == 2 ? A.new_lo : A.acc_hi) + qoff + e0;
+            const float* ps[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) ps[a] = a < NSRC ? srcb[a] + e0 : nullptr;
+            float* kq = A.kedge + 4 * eoff;
 #pragma unroll 1
             for (int cc = 0; cc < 4; ++cc) {
-                const int ce = e0 + cc * np;
                 const float qr = I.ref.q[cc];  // reference state (free-stream dissipation term)
                 float nxt[3][2][2];
                 if (cc < 3) {
@@ -342,10 +365,17 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         for (int j = 0; j < 2; ++j)
 #pragma unroll
                             for (int a = 0; a < 3; ++a)
-                                nxt[a][u][j] = (rok[u] && cok[j] && a < NSRC) ? __ldg(srcb[a] + (ce + np + off[u][j])) : 0.0f;
+                                nxt[a][u][j] = (rok[u] && cok[j] && a < NSRC) ? __ldg(ps[a] + np + u * nx + j) : 0.0f;
                 }
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+                float2 ey[2], ay[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+                if (!xi_closure && !eta_closure) {
+                    xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
+                    if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
+                    eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
+                    if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
+                } else {
                 if (!xi_closure) {
                     xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
                     if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
@@ -357,7 +387,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     }
                 }
                 // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
-                float2 ey[2], ay[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
                 if (!eta_closure) {
                     eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
                     if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
@@ -367,6 +396,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         ey[u] = eta_table<OPY, DIFF>(ecol + cc * YA, el[u], idxy, A.coef);
                         if constexpr (UPW) ay[u] = eta_table<OPY, DISS>(ecol + (4 + cc) * YA, el[u], idxy, A.coef);
                     }
+                }
                 }
 #pragma unroll
                 for (int u = 0; u < 2; ++u)
@@ -378,10 +408,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         float kc;
                         if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) * jinv[u][j] + qr * rinf[u][j];
                         else kc = (-exv - eyv) * jinv[u][j];
-                        const int e = ce + off[u][j];
+                        const int e = u * nx + j;
                         if (edge[u][j]) {
                             const int row = r0 + u, col = c0 + j;
-                            A.kedge[4 * (eoff + edge_index(row, col, nx, ny)) + cc] = kc;
+                            kq[4 * edge_index(row, col, nx, ny) + cc] = kc;
                         } else if constexpr (SC == 0) {
                             out1[e] = opn[0][u][j] + caf * kc;
                             out2[e] = cbf * kc;
@@ -395,6 +425,10 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                             out2[e] = lo;
                         }
                     }
+#pragma unroll
+                for (int a = 0; a < NSRC; ++a) ps[a] += np;
+                out1 += np;
+                out2 += np;
                 if (cc < 3) {
 #pragma unroll
                     for (int a = 0; a < NSRC; ++a)
