@@ -11,11 +11,12 @@ loop, device-synchronised) and "Total error: <e>" (--error, the sum over grids o
 against the initial-condition vortex), or with --output-json the same as one json line
 {"filename": ..., "time_elapsed": {"secs": s, "nanos": ns}, "error": e}.
 
-Differences: the snapshots go to a NumPy .npz file (the output path with its suffix replaced;
-per grid "<grid>/x", "<grid>/y" and "<grid>/rho", "<grid>/rhou", "<grid>/rhov", "<grid>/e" of
-shape (outputs, ny, nx)) because this environment has no HDF5 library; there is no progress
-bar; --distribute is accepted and changes nothing (every block of every grid already runs in
-one launch per stage); --precision f32c selects the compensated-f32 form.
+The output file (-o, default output.hdf) is HDF5 as the reference writes it: root dataset `t`
+(u64 step numbers of the outputs) and per grid a group with `x`, `y`, a soft link `t` -> `/t` and
+`rho`, `rhou`, `rhov`, `e` of shape (outputs, ny, nx), written by this package's own HDF5 writer
+(hdf5.py; contiguous, uncompressed datasets).  Differences: there is no progress bar;
+--distribute is accepted and changes nothing (every block of every grid already runs in one
+launch per stage); --precision f32c selects the compensated-f32 form.
 """
 from __future__ import annotations
 
@@ -29,6 +30,7 @@ import time
 import numpy as np
 
 from . import config as cfgmod
+from . import hdf5
 from . import multigrid as mg
 
 
@@ -55,24 +57,23 @@ def rust_display(x: float) -> str:
 
 
 class Snapshots:
+    """The output file of the run: the state of every grid at step 0, at every intermediate output
+    and at the end (System::output, multigrid/src/system.rs:591-616), written as HDF5 by
+    `hdf5.write_snapshots` when the run ends."""
+
     def __init__(self, path: str, names, grids):
-        root, _ = os.path.splitext(path)
-        self.path = root + ".npz"
+        self.path = path
         self.names = names
         self.grids = grids
+        self.times = []
         self.frames = []
 
-    def output(self, sys_):
+    def output(self, sys_, step: int):
+        self.times.append(step)
         self.frames.append([sys_.field(b) for b in range(len(self.names))])
 
     def write(self):
-        out = {}
-        for b, name in enumerate(self.names):
-            out[f"{name}/x"] = self.grids[b].x
-            out[f"{name}/y"] = self.grids[b].y
-            for c, comp in enumerate(("rho", "rhou", "rhov", "e")):
-                out[f"{name}/{comp}"] = np.stack([f[b][c] for f in self.frames])
-        np.savez(self.path, **out)
+        hdf5.write_snapshots(self.path, self.names, self.grids, self.times, self.frames)
 
 
 def main(argv=None) -> int:
@@ -103,7 +104,7 @@ def main(argv=None) -> int:
     s.set_dt(dt)
     ntime = int(round(rt.integration_time / dt))
     snaps = Snapshots(a.output, rt.names, rt.grids)
-    snaps.output(s)
+    snaps.output(s, 0)
     torch.cuda.synchronize(a.device)
     t0 = time.perf_counter()
     # main.rs:116-125: steps_between_outputs = max(n / ntime, 1) and the next output step is
@@ -114,10 +115,10 @@ def main(argv=None) -> int:
         s.advance(nexttime - itime)
         itime = nexttime
         if itime != ntime:
-            snaps.output(s)
+            snaps.output(s, itime)
     torch.cuda.synchronize(a.device)
     elapsed = time.perf_counter() - t0
-    snaps.output(s)
+    snaps.output(s, ntime)
     snaps.write()
     err = s.error() if a.error else None
     if a.output_json:

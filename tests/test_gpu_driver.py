@@ -33,7 +33,7 @@ CONFIG = """{
 
 
 def test_driver_matches_oracle(orc, tmp_path, capsys):
-    from summationbyparts_b200 import config, main, multigrid
+    from summationbyparts_b200 import config, hdf5, main, multigrid
     from summationbyparts_b200.system import BlockSpec
     path = tmp_path / "interp.json5"
     path.write_text(CONFIG)
@@ -41,7 +41,7 @@ def test_driver_matches_oracle(orc, tmp_path, capsys):
     assert main.main([str(path), "-o", str(out), "--error", "--timings", "--output-json"]) == 0
     info = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert info["filename"] == str(out) and "secs" in info["time_elapsed"]
-    snaps = np.load(str(tmp_path / "run.npz"))
+    snaps = hdf5.read_flat(str(out))
     assert snaps["grid1/rho"].shape == (2, 50, 99)
 
     rt = config.into_runtime(config.loads(CONFIG))
@@ -51,6 +51,8 @@ def test_driver_matches_oracle(orc, tmp_path, capsys):
     o.init_vortex(0.0)
     dt = o.max_dt()
     ntime = int(round(rt.integration_time / dt))
+    np.testing.assert_array_equal(snaps["t"], [0, ntime])  # step numbers of the outputs
+    np.testing.assert_array_equal(snaps["grid1/t"], snaps["t"])  # the soft link t -> /t
     o.advance(ntime, dt)
     assert abs(info["error"] - o.error()) <= 1e-10 * o.error()
     assert np.max(np.abs(snaps["grid0/rho"][1] - o.state(0)[0])) <= 1e-12 * np.max(np.abs(o.state(0)[0]))
@@ -84,14 +86,14 @@ def test_driver_expression_initial_conditions(orc, tmp_path, capsys):
     """Expression initial conditions through the command-line entry point: the state matches the
     oracle started from the same evaluated fields, and --error is the h2 error against the
     expressions at the final time (an advected density wave, exact on a periodic domain)."""
-    from summationbyparts_b200 import config, main, multigrid
+    from summationbyparts_b200 import config, hdf5, main, multigrid
     from summationbyparts_b200.system import BlockSpec
     path = tmp_path / "wave.json5"
     path.write_text(EXPR_CONFIG)
     out = tmp_path / "run.hdf"
     assert main.main([str(path), "-o", str(out), "--error", "--output-json"]) == 0
     info = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
-    snaps = np.load(str(tmp_path / "run.npz"))
+    snaps = hdf5.read_flat(str(out))
 
     rt = config.into_runtime(config.loads(EXPR_CONFIG))
     g = rt.grids[0]

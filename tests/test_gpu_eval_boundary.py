@@ -117,7 +117,7 @@ VORTEX_CONFIG = """{
 def test_driver_expression_boundaries(tmp_path, capsys):
     """The same vortex as expressions (initial and boundary conditions) and as the built-in vortex:
     same final state and the same --error through the command-line entry point."""
-    from summationbyparts_b200 import main
+    from summationbyparts_b200 import hdf5, main
     res = []
     for name, cfg in (("expr", EVAL_CONFIG), ("vortex", VORTEX_CONFIG)):
         path = tmp_path / f"{name}.json5"
@@ -125,7 +125,7 @@ def test_driver_expression_boundaries(tmp_path, capsys):
         out = tmp_path / f"{name}.hdf"
         assert main.main([str(path), "-o", str(out), "--error", "--output-json"]) == 0
         info = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
-        snaps = np.load(str(tmp_path / f"{name}.npz"))
+        snaps = hdf5.read_flat(str(tmp_path / f"{name}.hdf"))
         res.append((info["error"], snaps["grid/rho"][-1]))
     (e1, r1), (e2, r2) = res
     assert np.max(np.abs(r1 - r2)) <= 1e-12 * np.max(np.abs(r2))

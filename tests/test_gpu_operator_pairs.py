@@ -135,7 +135,7 @@ MIX_CONFIG = {
 
 def test_driver_mixed_operators(orc, tmp_path, capsys):
     """The multigrid driver on a four-block layout whose blocks use pairs of different families."""
-    from summationbyparts_b200 import config, main, multigrid
+    from summationbyparts_b200 import config, hdf5, main, multigrid
     from summationbyparts_b200.system import BlockSpec
     text = json.dumps(MIX_CONFIG)
     path = tmp_path / "mix.json"
@@ -143,7 +143,7 @@ def test_driver_mixed_operators(orc, tmp_path, capsys):
     out = tmp_path / "run.hdf"
     assert main.main([str(path), "-o", str(out), "--error", "--output-json"]) == 0
     info = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
-    snaps = np.load(str(tmp_path / "run.npz"))
+    snaps = hdf5.read_flat(str(tmp_path / "run.hdf"))
 
     rt = config.into_runtime(config.loads(text))
     ids = [g.op.ids for g in rt.grids]
