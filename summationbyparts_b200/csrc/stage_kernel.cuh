@@ -73,6 +73,7 @@ struct StageArgs {
     const float* rinf;       // compensated f32, upwind: free-stream dissipation planes (BlockDev::r_off)
     const double* xy;        // coordinates
     const T* coef;           // operator tables, see coef_base
+    const float4* pair;      // compensated f32: output-pair class tables (pair_row, stage_kernel_vec.cuh)
     double gamma;
     unsigned* status;
 };

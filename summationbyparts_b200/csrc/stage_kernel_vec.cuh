@@ -98,69 +98,67 @@ __device__ __forceinline__ void eta_pair(const float* __restrict__ p, float idx,
     out[1] = fmul2s(a1, idx);
 }
 
-// Table row, first input and tap count of output i of a length-n line (closure or interior).
-template <int OP>
-__device__ __forceinline__ void table_row(int i, int n, int& row, int& base, int& ntaps) {
-    constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N, D = OpShape<OP>::D, H = OpShape<OP>::H;
-    if (i < M) {
-        row = i;
-        base = 0;
-        ntaps = N;
-    } else if (i >= n - M) {
-        row = M + i - (n - M);
-        base = n - N;
-        ntaps = N;
-    } else {
-        row = 2 * M;
-        base = i - H;
-        ntaps = D;
+// Output pairs with a boundary closure.  A thread's two outputs along a line (columns c0, c0 + 1
+// for xi, rows r0, r0 + 1 for eta; c0 and r0 are even) fall into one of 1.5 M + 2 classes:
+// interior (class 0), both in the start closure (classes 1 .. M/2, by i0 / 2), or near the end
+// (classes M/2 + d for d = n - i0 = 1 .. M + 1: d <= M both in the end closure, or only i0 + 1
+// when d = 1 is past the end; d = M + 1 the first interior and the second in the closure).  For
+// every class the two outputs read inside one window of W consecutive inputs starting at s, and a
+// class's table holds, for each window position k, the pair coefficient (p_k, p_k, q_k, q_k) of
+// output 0 and output 1 (zero where a row has no tap).  So every thread of a closure tile or of a
+// closure row pair runs the same W-tap loop of paired FMAs -- no divergence, no per-tap tests --
+// and only its table row and window start depend on its class.  The coefficients are the f32
+// closure and interior rows of the table path, in the same tap order, so the sums are the same.
+constexpr int kPairW = 14;        // max W over the operators (Upwind9)
+constexpr int kPairClasses = 14;  // max 1.5 M + 2 over the operators
+__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int pair_window(int M, int N, int D, int H) { return imax(imax(D + 1, N), M + H + 1); }
+__host__ __device__ constexpr int pair_classes(int M) { return M + M / 2 + 2; }
+
+// Class of the output pair (i0, i0 + 1) of a length-n line (i0 even, i0 < n, n >= 2 M) and the
+// first input s of its window.
+__host__ __device__ __forceinline__ int pair_class(int M, int N, int H, int i0, int n, int& s) {
+    if (i0 < M) {
+        s = 0;
+        return 1 + i0 / 2;
     }
+    const int d = n - i0;
+    if (d <= M + 1) {
+        s = d == M + 1 ? (i0 - H < n - N ? i0 - H : n - N) : n - N;
+        return M / 2 + d;
+    }
+    s = i0 - H;
+    return 0;
+}
+template <int OP>
+__device__ __forceinline__ int pair_class(int i0, int n, int& s) {
+    return pair_class(OpShape<OP>::M, OpShape<OP>::N, OpShape<OP>::H, i0, n, s);
+}
+template <int OP>
+__device__ __forceinline__ bool closure_pair(int i0, int n) {
+    return i0 < OpShape<OP>::M || i0 + 1 >= n - OpShape<OP>::M;
 }
 
-// Closure-tile descriptors of one output line (a column for xi, a row for eta), computed once
-// per tile: the coefficient row's offset in the operator's table part, the shared-memory
-// offsets of the first even and odd tap (xi: transposed slots; eta: rows, `eb`) and the tap
-// count (N for closure rows, D for interior ones).
-struct TableLine {
-    int crow, te, to, ntaps;
-};
-
-// Xi sum of one kind over the thread's two rows, table path of stage_kernel (first product, then
-// the fma chain): arr = transposed array at row r0.
-template <int OP, int KIND>
-__device__ __forceinline__ float2 xi_table(const float* __restrict__ arr, const TableLine& L, float idx,
-                                           const float* __restrict__ ctab) {
-    constexpr int N = OpShape<OP>::N, NV = (N + 3) / 4;
-    const float* crow = ctab + coef_base(OP, KIND) + L.crow;
-    float cf[NV * 4];
+// Sums of one kind for an output pair of any class: ld(k) is the input pair at window position
+// k, cf the class's table row (W entries).
+template <int OP, class LD>
+__device__ __forceinline__ void pair_sums(const LD& ld, const float4* __restrict__ cf, float idx, float2 out[2]) {
+    constexpr int W = pair_window(OpShape<OP>::M, OpShape<OP>::N, OpShape<OP>::D, OpShape<OP>::H);
+    float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(cf + 4 * v) = __ldg(reinterpret_cast<const float4*>(crow) + v);
-    const float* pe = arr + L.te;  // taps 0, 2, 4, ...
-    const float* po = arr + L.to;  // taps 1, 3, 5, ...
-    float2 t = fmul2s(*reinterpret_cast<const float2*>(pe), cf[0]);
-#pragma unroll
-    for (int k = 1; k < N; ++k)
-        if (k < L.ntaps)
-            t = ffma2(*reinterpret_cast<const float2*>((k & 1 ? po : pe) + (k >> 1) * kVecPitch), cf[k], t);
-    return fmul2s(t, idx);
+    for (int k = 0; k < W; ++k) {
+        const float2 v = ld(k);
+        const float4 c = __ldg(cf + k);
+        a0 = __ffma2_rn(v, make_float2(c.x, c.y), a0);
+        a1 = __ffma2_rn(v, make_float2(c.z, c.w), a1);
+    }
+    out[0] = fmul2s(a0, idx);
+    out[1] = fmul2s(a1, idx);
 }
 
-// Eta sum of one kind over the thread's two columns, table path of stage_kernel (fma chain from
-// zero): col = eta array at local row 0, column c0; the taps are rows L.te + k.
-template <int OP, int KIND>
-__device__ __forceinline__ float2 eta_table(const float* __restrict__ col, const TableLine& L, float idx,
-                                            const float* __restrict__ ctab) {
-    constexpr int N = OpShape<OP>::N, NV = (N + 3) / 4;
-    const float* crow = ctab + coef_base(OP, KIND) + L.crow;
-    float cf[NV * 4];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(cf + 4 * v) = __ldg(reinterpret_cast<const float4*>(crow) + v);
-    const float* p = col + L.te;
-    float2 t = make_float2(0.0f, 0.0f);
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-        if (k < L.ntaps) t = ffma2(*reinterpret_cast<const float2*>(p + k * kTileX), cf[k], t);
-    return fmul2s(t, idx);
+// Table row of class `cls` for operator op and kind (DIFF, DISS) in the pair table.
+__device__ __forceinline__ const float4* pair_row(const float4* pair, int op, int kind, int cls) {
+    return pair + ((2 * op + kind) * kPairClasses + cls) * kPairW;
 }
 
 template <int OPX, int OPY>
@@ -196,6 +194,14 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     if (A.stage == kStageK || vec_stage_class(A.stage) != SC) {  // launched for another stage class
         if (tid == 0) atomicOr(A.status, STATUS_BAD_LAUNCH);
         return;
+    }
+    // Every shared array starts at zero: a pair-class window may reach slots that no tile of this
+    // CTA has written (their coefficients are zero), and those must hold finite values.
+    {
+        float4* z = reinterpret_cast<float4*>(smem_raw);
+        constexpr int n4 = (int)(vec_stage_smem<OPX, OPY>(UPW) / sizeof(float4));
+        for (int i = tid; i < n4; i += kStageThreads) z[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        __syncthreads();
     }
     // RK operand arrays (stage_operands): stage 0 u_in; stages 1, 2 acc_hi, prev_hi; stage 3 also prev_lo
     constexpr int NSRC = SC + 1;
@@ -307,10 +313,12 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 
         // ---------------- phase 2: stencils and stage update ----------------
         if (active) {
+            // xi: tiles holding closure columns run the pair-class path on every thread (the class
+            // follows the thread's column pair); eta: warps holding a closure row pair (warp w has
+            // row pairs 2 w, 2 w + 1) run it with each thread's own class (warp-uniform choice)
             const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
-            // eta: the table path only for threads holding a closure row (warps of 4 rows, so
-            // at most one warp per block end diverges); their windows lie inside the region
-            const bool eta_closure = r0 < OpShape<OPY>::M || r0 + 1 >= ny - OpShape<OPY>::M;
+            const int wr = y0 + 4 * (tid >> 5);  // first row of the warp
+            const bool eta_closure = closure_pair<OPY>(wr, ny) || (wr + 2 < ny && closure_pair<OPY>(wr + 2, ny));
             const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
             const float* xwe = xrow + xslot<XCH>(c0 - HX - lx0) * kVecPitch;      // ... column c0 - H
             const float* xwo = xrow + xslot<XCH>(c0 - HX - lx0 + 1) * kVecPitch;  // ... column c0 - H + 1
@@ -322,29 +330,23 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll
                 for (int j = 0; j < 2; ++j)
                     edge[u][j] = r0 + u == 0 || r0 + u == ny - 1 || c0 + j == 0 || c0 + j == nx - 1;
-            // table-path descriptors of the thread's columns (xi closure tiles) and rows (eta closure
-            // tiles); an output past the tile repeats the first one
-            TableLine xl[2], el[2];
+            // pair-class windows and table rows (closure tiles and warps only)
+            const float *gxe = xwe, *gxo = xwo, *gy = ewin;
+            const float4 *cfx = nullptr, *cfy = nullptr;
             if (xi_closure) {
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                int trow, base;
-                table_row<OPX>(cok[j] ? c0 + j : c0, nx, trow, base, xl[j].ntaps);
-                xl[j].crow = trow * kCoefRow;
-                xl[j].te = xslot<XCH>(base - lx0) * kVecPitch;
-                xl[j].to = xslot<XCH>(base - lx0 + 1) * kVecPitch;
-            }
+                int sx;
+                const int cls = pair_class<OPX>(c0, nx, sx);
+                gxe = xrow + xslot<XCH>(sx - lx0) * kVecPitch;
+                gxo = xrow + xslot<XCH>(sx - lx0 + 1) * kVecPitch;
+                cfx = pair_row(A.pair, OPX, DIFF, cls);
             }
             if (eta_closure) {
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                int trow, base;
-                table_row<OPY>(rok[u] ? r0 + u : r0, ny, trow, base, el[u].ntaps);
-                el[u].crow = trow * kCoefRow;
-                el[u].te = (base - ly0) * kTileX;
-                el[u].to = 0;
+                int sy;
+                const int cls = pair_class<OPY>(r0, ny, sy);
+                gy = ecol + (sy - ly0) * kTileX;
+                cfy = pair_row(A.pair, OPY, DIFF, cls);
             }
-            }
+            constexpr int kDissRow = kPairClasses * kPairW;  // DISS rows follow the DIFF rows of an operator
             // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
             // per-array pointers at point (r0, c0) of component cc, advanced by one plane per
             // component: the four points are at offsets 0, 1, nx, nx + 1
@@ -376,27 +378,33 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
                     if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
                 } else {
-                if (!xi_closure) {
-                    xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
-                    if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) {
-                        ex[j] = xi_table<OPX, DIFF>(xrow + cc * XA, xl[j], idxx, A.coef);
-                        if constexpr (UPW) dx[j] = xi_table<OPX, DISS>(xrow + (4 + cc) * XA, xl[j], idxx, A.coef);
+                    if (!xi_closure) {
+                        xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
+                        if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
+                    } else {
+                        // window position k = column sx + k: slots alternate between the two parities
+                        const float *pe = gxe + cc * XA, *po = gxo + cc * XA;
+                        pair_sums<OPX>([&](int k) { return *reinterpret_cast<const float2*>((k & 1 ? po : pe) + (k >> 1) * kVecPitch); },
+                                       cfx, idxx, ex);
+                        if constexpr (UPW) {
+                            const float *qe = pe + 4 * XA, *qo = po + 4 * XA;
+                            pair_sums<OPX>([&](int k) { return *reinterpret_cast<const float2*>((k & 1 ? qo : qe) + (k >> 1) * kVecPitch); },
+                                           cfx + kDissRow, idxx, dx);
+                        }
                     }
-                }
-                // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
-                if (!eta_closure) {
-                    eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
-                    if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
-                } else {
-#pragma unroll
-                    for (int u = 0; u < 2; ++u) {
-                        ey[u] = eta_table<OPY, DIFF>(ecol + cc * YA, el[u], idxy, A.coef);
-                        if constexpr (UPW) ay[u] = eta_table<OPY, DISS>(ecol + (4 + cc) * YA, el[u], idxy, A.coef);
+                    // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
+                    if (!eta_closure) {
+                        eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
+                        if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
+                    } else {
+                        const float* pw = gy + cc * YA;
+                        pair_sums<OPY>([&](int k) { return *reinterpret_cast<const float2*>(pw + k * kTileX); }, cfy, idxy, ey);
+                        if constexpr (UPW) {
+                            const float* qw = pw + 4 * YA;
+                            pair_sums<OPY>([&](int k) { return *reinterpret_cast<const float2*>(qw + k * kTileX); }, cfy + kDissRow,
+                                           idxy, ay);
+                        }
                     }
-                }
                 }
 #pragma unroll
                 for (int u = 0; u < 2; ++u)

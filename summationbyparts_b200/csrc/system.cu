@@ -160,6 +160,7 @@ struct sbp_system {
     double* d_sums = nullptr;
     unsigned long long* d_speeds = nullptr;
     void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
+    float4* d_pair = nullptr;  // compensated f32: output-pair class tables of the micro-tile kernel
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
@@ -230,7 +231,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf,    s->d_pair};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -308,6 +309,53 @@ void set_reference(InstanceDev& I, double gamma) {
     R.g_rho = float(gamma / rho);
 }
 
+// Output-pair class tables of the micro-tile kernel (pair_class, stage_kernel_vec.cuh), from the
+// f32 coefficient table `coef` (layout of coef_base): for every operator, kind and class, the W
+// window positions' (p, p, q, q), p the coefficient output 0 of the pair applies to the input at
+// that position and q output 1's, zero where the output's row has no tap.
+constexpr int kPairTableEntries = 12 * kPairClasses * kPairW;
+bool pair_table(const float* coef, std::vector<float4>& out) {
+    out.assign(kPairTableEntries, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    for (int op = 0; op < 6; ++op) {
+        OpInfo oi;
+        op_info(op, oi);
+        const int M = oi.M, N = oi.N, D = oi.D, H = (D - 1) / 2;
+        const int W = pair_window(M, N, D, H), ncls = pair_classes(M);
+        const int n = 1000;  // any line long enough: the classes depend on positions relative to its ends
+        // table row, first input and tap count of output i (table_row of the table path)
+        auto row_of = [&](int i, int& row, int& base, int& ntaps) {
+            if (i < M) {
+                row = i, base = 0, ntaps = N;
+            } else if (i >= n - M) {
+                row = M + i - (n - M), base = n - N, ntaps = N;
+            } else {
+                row = 2 * M, base = i - H, ntaps = D;
+            }
+        };
+        for (int cls = 0; cls < ncls; ++cls) {
+            const int i0 = cls == 0 ? 100 : (cls <= M / 2 ? 2 * (cls - 1) : n - (cls - M / 2));
+            int s0 = 0;
+            if (pair_class(M, N, H, i0, n, s0) != cls) return false;  // the class numbering above
+            for (int kind = 0; kind < (oi.upwind ? 2 : 1); ++kind) {
+                const float* tab = coef + (2 * op + kind) * kCoefStride;
+                float4* dst = out.data() + ((2 * op + kind) * kPairClasses + cls) * kPairW;
+                for (int o = 0; o < 2 && i0 + o < n; ++o) {
+                    int row, base, ntaps;
+                    row_of(i0 + o, row, base, ntaps);
+                    for (int t = 0; t < ntaps; ++t) {
+                        const int k = base + t - s0;
+                        if (k < 0 || k >= W) return false;  // the window covers every tap
+                        const float c = tab[row * kCoefRow + t];
+                        if (o == 0) dst[k].x = dst[k].y = c;
+                        else dst[k].z = dst[k].w = c;
+                    }
+                }
+            }
+        }
+    }
+    return true;
+}
+
 template <class T>
 StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     StageArgs<T> a{};
@@ -333,6 +381,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.rinf = s->rinf;
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
+    a.pair = s->d_pair;
     a.kedge = static_cast<T*>(s->kedge);
     a.mg = s->d_mg;
     a.eval = s->d_eval;
@@ -988,6 +1037,7 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_sums, (size_t)nblocks * (1 + kNormParts) * sizeof(double));
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
+    if (s->prec == 1) e = e ?: alloc((void**)&s->d_pair, kPairTableEntries * sizeof(float4));
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
     e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
     e = e ?: alloc((void**)&s->d_eval, sizeof(EvalDev));
@@ -1009,6 +1059,15 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     std::vector<double> coef_host(12 * kCoefStride);  // large enough for either precision
     fill_coef_table(s->prec, coef_host.data(), kCoefStride, kCoefRow);
     e = e ?: cudaMemcpyAsync(s->d_coef, coef_host.data(), 12 * kCoefStride * ts, cudaMemcpyHostToDevice, st);
+    std::vector<float4> pair_host;
+    if (s->prec == 1) {
+        if (!pair_table(reinterpret_cast<const float*>(coef_host.data()), pair_host)) {
+            set_error("internal: output-pair class table does not cover the operators' taps");
+            return fail(SBP_ERR_INVALID_ARGUMENT);
+        }
+        e = e ?: cudaMemcpyAsync(s->d_pair, pair_host.data(), kPairTableEntries * sizeof(float4), cudaMemcpyHostToDevice,
+                                 st);
+    }
     {
         std::vector<int64_t> p8(nblocks);
         for (int b = 0; b < nblocks; ++b) p8[b] = 2 * s->dense_off[b];
