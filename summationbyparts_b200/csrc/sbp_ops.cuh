@@ -94,15 +94,17 @@ SBP_COEF_ALL_DISS(UPWIND9H2, UPWIND9H2)
 #undef SBP_COEF_ALL_DISS
 
 
-// The interior diagonals in f32 as compile-time constants (the same literals as the constant
-// tables): the paired-FMA stencils of the micro-tile kernel take their coefficients from here, so
-// each tap's coefficient is an immediate and the zero tap of a central difference is skipped.
+// The interior diagonals (v) and start-closure blocks (st, M x N by rows) in f32 as
+// compile-time constants (the same literals as the constant tables): the micro-tile kernel takes
+// its stencil coefficients from here, so each tap's coefficient is an immediate and the zero tap
+// of a central difference is skipped.
 template <int OP, int KIND>
 struct CDiag;
-#define SBP_CD(OP, TAG, KINDV, KINDN)                                           \
-    template <>                                                                  \
-    struct CDiag<OP, KINDV> {                                                    \
-        static constexpr float v[] = {SBPC_##TAG##_##KINDN##_DIAG(SBPC_LIT_F32)}; \
+#define SBP_CD(OP, TAG, KINDV, KINDN)                                              \
+    template <>                                                                     \
+    struct CDiag<OP, KINDV> {                                                       \
+        static constexpr float v[] = {SBPC_##TAG##_##KINDN##_DIAG(SBPC_LIT_F32)};   \
+        static constexpr float st[] = {SBPC_##TAG##_##KINDN##_START(SBPC_LIT_F32)}; \
     };
 SBP_CD(UPWIND4, UPWIND4, DIFF, DIFF)
 SBP_CD(UPWIND4H2, UPWIND4H2, DIFF, DIFF)

@@ -161,10 +161,64 @@ __device__ __forceinline__ const float4* pair_row(const float4* pair, int op, in
     return pair + ((2 * op + kind) * kPairClasses + cls) * kPairW;
 }
 
+// Closure-column xi terms of a tile (closure_xi): [component][closure column][row], row pitch 34.
+constexpr int kClosurePitch = 34;
+
 template <int OPX, int OPY>
 constexpr size_t vec_stage_smem(bool upw) {
     using G = VecGeom<OPX, OPY>;
-    return sizeof(float) * (size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1);
+    return sizeof(float) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * OpShape<OPX>::M * kClosurePitch);
+}
+
+// Closure-block coefficient (row I, input K) of one end of a line: the start block, or the end
+// block (row I applies -/+ st[(M - 1 - I) N + (N - 1 - K)], DIFF negated).
+template <int OP, int KIND, bool RIGHT, int I, int K>
+struct ClosureCoef {
+    static constexpr int M = OpShape<OP>::M, N = OpShape<OP>::N;
+    static constexpr float value = RIGHT ? (KIND == DIFF ? -1.0f : 1.0f) * CDiag<OP, KIND>::st[(M - 1 - I) * N + (N - 1 - K)]
+                                         : CDiag<OP, KIND>::st[I * N + K];
+};
+// Rows I.. of the closure block: the sum over the N inputs v, first product then an fma chain
+// (the table path's order).
+template <int OP, int KIND, bool RIGHT, int I, int K = 1>
+__device__ __forceinline__ float closure_sum(const float* v, float t) {
+    if constexpr (K == 1) t = v[0] * ClosureCoef<OP, KIND, RIGHT, I, 0>::value;
+    if constexpr (K < OpShape<OP>::N) {
+        constexpr float c = ClosureCoef<OP, KIND, RIGHT, I, K>::value;
+        return closure_sum<OP, KIND, RIGHT, I, K + 1>(v, __fmaf_rn(v[K], c, t));
+    } else {
+        return t;
+    }
+}
+
+// Writes closure columns I .. I + CNT - 1 of closure_xi.
+template <int OP, bool UPW, bool RIGHT, int I, int CNT>
+__device__ __forceinline__ void closure_out(const float* ve, const float* va, float idx, float* cb) {
+    if constexpr (CNT > 0) {
+        float d = 0.0f;
+        if constexpr (UPW) d = closure_sum<OP, DISS, RIGHT, I>(va, 0.0f) * idx;
+        cb[I * kClosurePitch] = d - closure_sum<OP, DIFF, RIGHT, I>(ve, 0.0f) * idx;
+        closure_out<OP, UPW, RIGHT, I + 1, CNT - 1>(ve, va, idx, cb);
+    }
+}
+
+// The xi term diss_xi(alpha_u q) - diff_xi(Ehat) of closure columns I0 .. I0 + CNT - 1 at one end
+// of a line, for one component and tile row: e / a are the transposed Ehat / alpha_u q arrays at
+// the row, `lc` the local column of the block's first input; each sum scaled by idx as the
+// interior path scales it, into cb[i * kClosurePitch].
+template <int OP, bool UPW, bool RIGHT, int XCH, int I0, int CNT>
+__device__ __forceinline__ void closure_xi(const float* __restrict__ e, const float* __restrict__ a, int lc, float idx,
+                                           float* __restrict__ cb) {
+    constexpr int N = OpShape<OP>::N;
+    const int se = xslot<XCH>(lc) * kVecPitch, so = xslot<XCH>(lc + 1) * kVecPitch;
+    float ve[N], va[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const int o = (k & 1 ? so : se) + (k >> 1) * kVecPitch;
+        ve[k] = e[o];
+        va[k] = UPW ? a[o] : 0.0f;
+    }
+    closure_out<OP, UPW, RIGHT, I0, CNT>(ve, va, idx, cb);
 }
 
 // Stage class of the RK update: 0 = stage 0, 1 = stages 1 and 2, 2 = stage 3.  The micro-tile
@@ -181,12 +235,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     constexpr int HX = OpShape<OPX>::H, HY = OpShape<OPY>::H;
     // phase-1 points per thread and batch: enough for an interior tile's whole region
     // ((32 + 2 H_eta) rows x 32 + 32 rows x 2 H_xi points) in one batch of loads
-    // phase-1 points per thread and batch: enough for an interior tile's whole region
-    // ((32 + 2 H_eta) rows x 32 + 32 rows x 2 H_xi points) in one batch of loads
     constexpr int P1B = ((kVecRows + 2 * HY) * kTileX + kVecRows * 2 * HX + kStageThreads - 1) / kStageThreads;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sE = reinterpret_cast<float*>(smem_raw);  // [UPW ? 8 : 4][2 XCH][34]: Ehat, alpha_u q (transposed)
     float* sF = sE + (UPW ? 8 : 4) * XA;             // [UPW ? 8 : 4][HYP][32]: Fhat, alpha_v q
+    float* cbuf = sF + (UPW ? 8 : 4) * YA;           // [4][M_xi][34]: closure-column xi terms
     const float gamma = float(A.gamma);
     const int tid = threadIdx.x;
     const int grp = tid & 15, rpr = tid >> 4;  // column pair, row pair (0..15 each)
@@ -311,17 +364,47 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
             }
         __syncthreads();
 
+        // A tile holding the closure columns of one end of its rows: their xi sums for every row
+        // and array go to cbuf first (all threads, one barrier) and replace, in phase 2, what the
+        // interior path computes for those columns.  A tile holding both ends (rows shorter than
+        // a tile and a half) takes the pair-class path instead.
+        const bool left_cl = x0 < OpShape<OPX>::M, right_cl = x1 > nx - OpShape<OPX>::M;
+        const bool one_end = left_cl != right_cl;
+        if (one_end) {
+            // thread: component tid / 64, tile row (tid / 2) % 32, half tid % 2 of the M columns
+            constexpr int MX = OpShape<OPX>::M;
+            const int comp = tid >> 6, r = (tid >> 1) & 31, half = tid & 1;
+            if (r < th) {
+                const int lc = right_cl ? nx - OpShape<OPX>::N - lx0 : -lx0;
+                const float* e = sE + comp * XA + r;
+                const float* al = sE + (UPW ? 4 + comp : comp) * XA + r;
+                float* cb = cbuf + comp * MX * kClosurePitch + r;
+                if (right_cl) {
+                    if (half) closure_xi<OPX, UPW, true, XCH, MX / 2, MX / 2>(e, al, lc, idxx, cb);
+                    else closure_xi<OPX, UPW, true, XCH, 0, MX / 2>(e, al, lc, idxx, cb);
+                } else {
+                    if (half) closure_xi<OPX, UPW, false, XCH, MX / 2, MX / 2>(e, al, lc, idxx, cb);
+                    else closure_xi<OPX, UPW, false, XCH, 0, MX / 2>(e, al, lc, idxx, cb);
+                }
+            }
+            __syncthreads();
+        }
+
         // ---------------- phase 2: stencils and stage update ----------------
         if (active) {
-            // xi: tiles holding closure columns run the pair-class path on every thread (the class
-            // follows the thread's column pair); eta: warps holding a closure row pair (warp w has
-            // row pairs 2 w, 2 w + 1) run it with each thread's own class (warp-uniform choice)
-            const bool xi_closure = x0 < OpShape<OPX>::M || x1 > nx - OpShape<OPX>::M;
+            // xi: tiles holding both ends' closure columns run the pair-class path on every thread
+            // (the class follows the thread's column pair); eta: warps holding a closure row pair
+            // (warp w has row pairs 2 w, 2 w + 1) run it with each thread's own class
+            // (warp-uniform choice)
+            const bool xi_closure = left_cl && right_cl;
             const int wr = y0 + 4 * (tid >> 5);  // first row of the warp
             const bool eta_closure = closure_pair<OPY>(wr, ny) || (wr + 2 < ny && closure_pair<OPY>(wr + 2, ny));
             const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
-            const float* xwe = xrow + xslot<XCH>(c0 - HX - lx0) * kVecPitch;      // ... column c0 - H
-            const float* xwo = xrow + xslot<XCH>(c0 - HX - lx0 + 1) * kVecPitch;  // ... column c0 - H + 1
+            // interior-path window from column c0 - H (kept inside the arrays for closure columns,
+            // whose interior-path sums are replaced)
+            const int cw = min(max(c0 - HX - lx0, 0), G::XC - OpShape<OPX>::D - 1);
+            const float* xwe = xrow + xslot<XCH>(cw) * kVecPitch;      // xi arrays at column c0 - H
+            const float* xwo = xrow + xslot<XCH>(cw + 1) * kVecPitch;  // ... column c0 - H + 1
             const float* ecol = sF + (c0 - x0);                        // eta arrays at local row 0, column c0
             const float* ewin = ecol + (r0 - HY - ly0) * kTileX;       // ... at row r0 - H
             bool edge[2][2];
@@ -403,6 +486,19 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                             const float* qw = pw + 4 * YA;
                             pair_sums<OPY>([&](int k) { return *reinterpret_cast<const float2*>(qw + k * kTileX); }, cfy + kDissRow,
                                            idxy, ay);
+                        }
+                    }
+                }
+                if (one_end) {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const int ci = left_cl ? c0 + j : c0 + j - (nx - OpShape<OPX>::M);
+                        if (ci >= 0 && ci < OpShape<OPX>::M && cok[j]) {
+                            // the whole xi term as -ex: (-ex - ey + dx) + ay with dx = 0
+                            const float2 t = *reinterpret_cast<const float2*>(
+                                cbuf + (cc * OpShape<OPX>::M + ci) * kClosurePitch + (r0 - y0));
+                            ex[j] = make_float2(-t.x, -t.y);
+                            dx[j] = make_float2(0.0f, 0.0f);
                         }
                     }
                 }
