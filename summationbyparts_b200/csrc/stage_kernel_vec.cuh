@@ -221,6 +221,18 @@ __device__ __forceinline__ void closure_xi(const float* __restrict__ e, const fl
     closure_out<OP, UPW, RIGHT, I0, CNT>(ve, va, idx, cb);
 }
 
+// The two values of a thread's row u at columns c0, c0 + 1 from `p` (the element of (r0, c0)).
+// Row r0 starts at an even element (r0 and c0 are even, planes start 256-byte aligned), so its
+// pair is one 8-byte load, which stays inside the plane's padded extent even where c0 + 1 is past
+// the row (the second value is then not used); row r0 + 1 is one 8-byte load for even nx, else
+// two loads.
+__device__ __forceinline__ float2 ld_row_pair(const float* __restrict__ p, int u, int nx, bool ok1, bool cok1, float def) {
+    if (u == 0) return __ldg(reinterpret_cast<const float2*>(p));
+    if (!ok1) return make_float2(def, def);
+    if ((nx & 1) == 0) return __ldg(reinterpret_cast<const float2*>(p + nx));
+    return make_float2(__ldg(p + nx), cok1 ? __ldg(p + nx + 1) : def);
+}
+
 // Stage class of the RK update: 0 = stage 0, 1 = stages 1 and 2, 2 = stage 3.  The micro-tile
 // kernel takes it as a template parameter, so the operand arrays it reads and the update it
 // writes are fixed at compile time (the k-only stage of other tableaus runs on f64 systems only).
@@ -340,28 +352,38 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 
         // Phase-2 operands of this thread (1 / J and component 0's RK operands), loaded before
         // the barrier so the loads overlap the other warps' phase 1.  Element of point (u, j)
-        // of component cc: in-block offset e0 + cc * np + off[u][j] from the block bases.
+        // of component cc: in-block offset e0 + cc * np + u * nx + j from the block bases.
         const int c0 = x0 + 2 * grp, r0 = y0 + 2 * rpr;
         const bool cok[2] = {2 * grp < tw, 2 * grp + 1 < tw};
         const bool rok[2] = {2 * rpr < th, 2 * rpr + 1 < th};
         const bool active = cok[0] && rok[0];
         const int e0 = r0 * nx + c0;
-        const int off[2][2] = {{0, 1}, {nx, nx + 1}};
         const float* srcb[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) srcb[a] = a < NSRC ? src[a] + qoff : nullptr;
         float jinv[2][2], rinf[2][2], opn[3][2][2];  // jinv: plane 0 of the f32 metrics, 1 / J
         const float* rb = UPW ? A.rinf + B.r_off : nullptr;
+        if (active) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u)
+            for (int u = 0; u < 2; ++u) {
+                const float2 jv = ld_row_pair(mt + e0, u, nx, rok[1], cok[1], 1.0f);
+                jinv[u][0] = jv.x;
+                jinv[u][1] = jv.y;
+                if constexpr (UPW) {
+                    const float2 rv = ld_row_pair(rb + e0, u, nx, rok[1], cok[1], 0.0f);
+                    rinf[u][0] = rv.x;
+                    rinf[u][1] = rv.y;
+                } else {
+                    rinf[u][0] = rinf[u][1] = 0.0f;
+                }
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const bool ok = rok[u] && cok[j];
-                jinv[u][j] = ok ? __ldg(mt + (e0 + off[u][j])) : 1.0f;
-                rinf[u][j] = (UPW && ok) ? __ldg(rb + (e0 + off[u][j])) : 0.0f;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) opn[a][u][j] = (ok && a < NSRC) ? __ldg(srcb[a] + (e0 + off[u][j])) : 0.0f;
+                for (int a = 0; a < 3; ++a) {
+                    const float2 ov = a < NSRC ? ld_row_pair(srcb[a] + e0, u, nx, rok[1], cok[1], 0.0f) : make_float2(0.0f, 0.0f);
+                    opn[a][u][0] = ov.x;
+                    opn[a][u][1] = ov.y;
+                }
             }
+        }
         __syncthreads();
 
         // A tile holding the closure columns of one end of its rows: their xi sums for every row
@@ -447,10 +469,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll
                     for (int u = 0; u < 2; ++u)
 #pragma unroll
-                        for (int j = 0; j < 2; ++j)
-#pragma unroll
-                            for (int a = 0; a < 3; ++a)
-                                nxt[a][u][j] = (rok[u] && cok[j] && a < NSRC) ? __ldg(ps[a] + np + u * nx + j) : 0.0f;
+                        for (int a = 0; a < 3; ++a) {
+                            const float2 v = a < NSRC ? ld_row_pair(ps[a] + np, u, nx, rok[1], cok[1], 0.0f) : make_float2(0.0f, 0.0f);
+                            nxt[a][u][0] = v.x;
+                            nxt[a][u][1] = v.y;
+                        }
                 }
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
@@ -503,32 +526,48 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < 2; ++u)
+                for (int u = 0; u < 2; ++u) {
+                    if (!rok[u]) continue;
+                    float v1[2], v2[2];
+                    bool st[2];
 #pragma unroll
                     for (int j = 0; j < 2; ++j) {
-                        if (!(rok[u] && cok[j])) continue;
                         const float exv = u == 0 ? ex[j].x : ex[j].y, dxv = u == 0 ? dx[j].x : dx[j].y;
                         const float eyv = j == 0 ? ey[u].x : ey[u].y, ayv = j == 0 ? ay[u].x : ay[u].y;
                         float kc;
                         if constexpr (UPW) kc = (-exv - eyv + dxv + ayv) * jinv[u][j] + qr * rinf[u][j];
                         else kc = (-exv - eyv) * jinv[u][j];
-                        const int e = u * nx + j;
-                        if (edge[u][j]) {
-                            const int row = r0 + u, col = c0 + j;
-                            kq[4 * edge_index(row, col, nx, ny) + cc] = kc;
-                        } else if constexpr (SC == 0) {
-                            out1[e] = opn[0][u][j] + caf * kc;
-                            out2[e] = cbf * kc;
+                        st[j] = cok[j] && !edge[u][j];
+                        if (cok[j] && edge[u][j]) kq[4 * edge_index(r0 + u, c0 + j, nx, ny) + cc] = kc;
+                        if constexpr (SC == 0) {
+                            v1[j] = opn[0][u][j] + caf * kc;
+                            v2[j] = cbf * kc;
                         } else if constexpr (SC == 1) {
-                            out1[e] = opn[1][u][j] + caf * kc;
-                            out2[e] = opn[0][u][j] + cbf * kc;
+                            v1[j] = opn[1][u][j] + caf * kc;
+                            v2[j] = opn[0][u][j] + cbf * kc;
                         } else {
                             float hi = opn[1][u][j], lo = opn[2][u][j];
                             comp_add(hi, lo, opn[0][u][j] + cbf * kc);
-                            out1[e] = hi;
-                            out2[e] = lo;
+                            v1[j] = hi;
+                            v2[j] = lo;
                         }
                     }
+                    // one 8-byte store per output array where both points are written and the
+                    // row's pair is 8-byte aligned (see ld_row_pair), else one store per point
+                    float* p1 = out1 + u * nx;
+                    float* p2 = out2 + u * nx;
+                    if (st[0] && st[1] && (u == 0 || (nx & 1) == 0)) {
+                        *reinterpret_cast<float2*>(p1) = make_float2(v1[0], v1[1]);
+                        *reinterpret_cast<float2*>(p2) = make_float2(v2[0], v2[1]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 2; ++j)
+                            if (st[j]) {
+                                p1[j] = v1[j];
+                                p2[j] = v2[j];
+                            }
+                    }
+                }
 #pragma unroll
                 for (int a = 0; a < NSRC; ++a) ps[a] += np;
                 out1 += np;
