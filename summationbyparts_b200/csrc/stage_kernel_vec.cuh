@@ -161,13 +161,18 @@ __device__ __forceinline__ const float4* pair_row(const float4* pair, int op, in
     return pair + ((2 * op + kind) * kPairClasses + cls) * kPairW;
 }
 
-// Closure-column xi terms of a tile (closure_xi): [component][closure column][row], row pitch 34.
+// Closure terms of a tile: xi ([component][closure column][row], row pitch 34, closure_xi) or
+// eta ([component][closure row][column], closure_eta), one at a time.
 constexpr int kClosurePitch = 34;
+__host__ __device__ constexpr int closure_buffer_elems(int mx, int my) {
+    return 4 * mx * kClosurePitch > 4 * my * kTileX ? 4 * mx * kClosurePitch : 4 * my * kTileX;
+}
+
 
 template <int OPX, int OPY>
 constexpr size_t vec_stage_smem(bool upw) {
     using G = VecGeom<OPX, OPY>;
-    return sizeof(float) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + 4 * OpShape<OPX>::M * kClosurePitch);
+    return sizeof(float) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + closure_buffer_elems(OpShape<OPX>::M, OpShape<OPY>::M));
 }
 
 // Closure-block coefficient (row I, input K) of one end of a line: the start block, or the end
@@ -192,13 +197,13 @@ __device__ __forceinline__ float closure_sum(const float* v, float t) {
 }
 
 // Writes closure columns I .. I + CNT - 1 of closure_xi.
-template <int OP, bool UPW, bool RIGHT, int I, int CNT>
+template <int OP, bool UPW, bool RIGHT, int I, int CNT, int PITCH = kClosurePitch>
 __device__ __forceinline__ void closure_out(const float* ve, const float* va, float idx, float* cb) {
     if constexpr (CNT > 0) {
         float d = 0.0f;
         if constexpr (UPW) d = closure_sum<OP, DISS, RIGHT, I>(va, 0.0f) * idx;
-        cb[I * kClosurePitch] = d - closure_sum<OP, DIFF, RIGHT, I>(ve, 0.0f) * idx;
-        closure_out<OP, UPW, RIGHT, I + 1, CNT - 1>(ve, va, idx, cb);
+        cb[I * PITCH] = d - closure_sum<OP, DIFF, RIGHT, I>(ve, 0.0f) * idx;
+        closure_out<OP, UPW, RIGHT, I + 1, CNT - 1, PITCH>(ve, va, idx, cb);
     }
 }
 
@@ -219,6 +224,23 @@ __device__ __forceinline__ void closure_xi(const float* __restrict__ e, const fl
         va[k] = UPW ? a[o] : 0.0f;
     }
     closure_out<OP, UPW, RIGHT, I0, CNT>(ve, va, idx, cb);
+}
+
+// The eta term diss_eta(alpha_v q) - diff_eta(Fhat) of closure rows I0 .. I0 + CNT - 1 at one
+// end of a column (BOTTOM = false: rows 0 .. M - 1, true: n - M .. n - 1), for one component and
+// tile column: f / a are the Fhat / alpha_v q arrays at the column, `lr` the local row of the
+// block's first input; each sum scaled by idx, into cb[i * kTileX].
+template <int OP, bool UPW, bool BOTTOM, int I0, int CNT>
+__device__ __forceinline__ void closure_eta(const float* __restrict__ f, const float* __restrict__ a, int lr, float idx,
+                                            float* __restrict__ cb) {
+    constexpr int N = OpShape<OP>::N;
+    float ve[N], va[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        ve[k] = f[(lr + k) * kTileX];
+        va[k] = UPW ? a[(lr + k) * kTileX] : 0.0f;
+    }
+    closure_out<OP, UPW, BOTTOM, I0, CNT, kTileX>(ve, va, idx, cb);
 }
 
 // The two values of a thread's row u at columns c0, c0 + 1 from `p` (the element of (r0, c0)).
@@ -251,7 +273,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sE = reinterpret_cast<float*>(smem_raw);  // [UPW ? 8 : 4][2 XCH][34]: Ehat, alpha_u q (transposed)
     float* sF = sE + (UPW ? 8 : 4) * XA;             // [UPW ? 8 : 4][HYP][32]: Fhat, alpha_v q
-    float* cbuf = sF + (UPW ? 8 : 4) * YA;           // [4][M_xi][34]: closure-column xi terms
+    float* cbuf = sF + (UPW ? 8 : 4) * YA;           // closure terms (closure_buffer_elems)
     const float gamma = float(A.gamma);
     const int tid = threadIdx.x;
     const int grp = tid & 15, rpr = tid >> 4;  // column pair, row pair (0..15 each)
@@ -411,6 +433,29 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
             }
             __syncthreads();
         }
+        // The same for a tile holding the closure rows of one end of its columns when the buffer
+        // is free (no xi closure): thread = component tid / 64, half (tid / 32) % 2 of the M rows,
+        // tile column tid % 32.  Other tiles with closure rows take the pair-class path.
+        const bool top_cl = y0 < OpShape<OPY>::M, bot_cl = y1 > ny - OpShape<OPY>::M;
+        const bool eta_pre = top_cl != bot_cl && !one_end;
+        if (eta_pre) {
+            constexpr int MY = OpShape<OPY>::M;
+            const int comp = tid >> 6, half = (tid >> 5) & 1, col = tid & 31;
+            if (col < tw) {
+                const int lr = bot_cl ? ny - OpShape<OPY>::N - ly0 : -ly0;
+                const float* f = sF + comp * YA + col;
+                const float* al = sF + (UPW ? 4 + comp : comp) * YA + col;
+                float* cb = cbuf + comp * MY * kTileX + col;
+                if (bot_cl) {
+                    if (half) closure_eta<OPY, UPW, true, MY / 2, MY / 2>(f, al, lr, idxy, cb);
+                    else closure_eta<OPY, UPW, true, 0, MY / 2>(f, al, lr, idxy, cb);
+                } else {
+                    if (half) closure_eta<OPY, UPW, false, MY / 2, MY / 2>(f, al, lr, idxy, cb);
+                    else closure_eta<OPY, UPW, false, 0, MY / 2>(f, al, lr, idxy, cb);
+                }
+            }
+            __syncthreads();
+        }
 
         // ---------------- phase 2: stencils and stage update ----------------
         if (active) {
@@ -420,7 +465,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
             // (warp-uniform choice)
             const bool xi_closure = left_cl && right_cl;
             const int wr = y0 + 4 * (tid >> 5);  // first row of the warp
-            const bool eta_closure = closure_pair<OPY>(wr, ny) || (wr + 2 < ny && closure_pair<OPY>(wr + 2, ny));
+            const bool eta_closure =
+                !eta_pre && (closure_pair<OPY>(wr, ny) || (wr + 2 < ny && closure_pair<OPY>(wr + 2, ny)));
             const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
             // interior-path window from column c0 - H (kept inside the arrays for closure columns,
             // whose interior-path sums are replaced)
@@ -428,7 +474,9 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
             const float* xwe = xrow + xslot<XCH>(cw) * kVecPitch;      // xi arrays at column c0 - H
             const float* xwo = xrow + xslot<XCH>(cw + 1) * kVecPitch;  // ... column c0 - H + 1
             const float* ecol = sF + (c0 - x0);                        // eta arrays at local row 0, column c0
-            const float* ewin = ecol + (r0 - HY - ly0) * kTileX;       // ... at row r0 - H
+            // interior-path window from row r0 - H (kept inside the arrays for closure rows, whose
+            // interior-path sums are replaced)
+            const float* ewin = ecol + min(max(r0 - HY - ly0, 0), G::HYP - OpShape<OPY>::D - 1) * kTileX;
             bool edge[2][2];
 #pragma unroll
             for (int u = 0; u < 2; ++u)
@@ -522,6 +570,18 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                                 cbuf + (cc * OpShape<OPX>::M + ci) * kClosurePitch + (r0 - y0));
                             ex[j] = make_float2(-t.x, -t.y);
                             dx[j] = make_float2(0.0f, 0.0f);
+                        }
+                    }
+                }
+                if (eta_pre) {
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int ri = top_cl ? r0 + u : r0 + u - (ny - OpShape<OPY>::M);
+                        if (ri >= 0 && ri < OpShape<OPY>::M && rok[u]) {
+                            const float2 t = *reinterpret_cast<const float2*>(
+                                cbuf + (cc * OpShape<OPY>::M + ri) * kTileX + (c0 - x0));
+                            ey[u] = make_float2(-t.x, -t.y);
+                            ay[u] = make_float2(0.0f, 0.0f);
                         }
                     }
                 }

@@ -75,7 +75,7 @@ size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
         const int xc = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
         const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
         return sizeof(float) *
-               ((size_t)(4 * 2 * ((xc + 1) / 2) * kVecPitch + 4 * hyp * kTileX) * (upw ? 2 : 1) + 4 * ox.M * kClosurePitch);
+               ((size_t)(4 * 2 * ((xc + 1) / 2) * kVecPitch + 4 * hyp * kTileX) * (upw ? 2 : 1) + closure_buffer_elems(ox.M, oy.M));
     }
     const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
     const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
