@@ -68,6 +68,11 @@ struct InstanceDev {
     // p 1/(gamma M^2)); f64 systems store the state itself.
     double qref[4];
     RefState ref;
+    // Per-vortex constants of vortex_point_fast (set with the reference state): the factor of
+    // e^f in 1 - K e^f, the factor of dx e^(f/2) and dy e^(f/2) in the velocity, 1 / r*^2; and
+    // the free-stream pressure and 1 / (gamma - 1).
+    double vk_b[5], vk_u[5], vk_f[5];
+    double v_pinf, v_igm1;
 };
 
 // pressure (euler/src/lib.rs:478-480)
@@ -129,6 +134,44 @@ __device__ inline void vortex_point(const InstanceDev& I, double gamma, double t
             q[1] += r * u - rho_inf * u_inf;
             q[2] += r * v - rho_inf * v_inf;
             q[3] += (p / (gamma - 1.0) + r * (u * u + v * v) / 2.0) - e_inf;
+        }
+    }
+}
+
+// vortex_point<true> for gamma = 1.4 with the instance constants precomputed on the host
+// (InstanceDev::vk_*) and no division: the boundary data of compensated-f32 systems, whose f64
+// SAT terms need not follow the reference's operation order (values differ in the last bits).
+__device__ inline void vortex_point_fast(const InstanceDev& I, double t, double x, double y, double q[4]) {
+    const double p_inf = I.v_pinf, igm1 = I.v_igm1;
+    const double e_inf = p_inf * igm1 + 0.5;  // rho_inf = u_inf = 1, v_inf = 0
+    if (I.nvort <= 0) {
+        q[0] = 1.0;
+        q[1] = 1.0;
+        q[2] = 0.0;
+        q[3] = e_inf;
+        return;
+    }
+    for (int iv = 0; iv < I.nvort; ++iv) {
+        const double dx = (x - I.x0[iv]) - t;
+        const double dy = y - I.y0[iv];
+        const double ef = exp((1.0 - (dx * dx + dy * dy)) * I.vk_f[iv]);
+        const double b = 1.0 - I.vk_b[iv] * ef;
+        const double sb = sqrt(b);
+        const double r = b * b * sb;
+        const double p = b * r * p_inf;
+        const double w = I.vk_u[iv] * sqrt(ef);
+        const double u = 1.0 - w * dy, v = w * dx;
+        const double en = p * igm1 + 0.5 * r * (u * u + v * v);
+        if (iv == 0) {
+            q[0] = r;
+            q[1] = r * u;
+            q[2] = r * v;
+            q[3] = en;
+        } else {
+            q[0] += r - 1.0;
+            q[1] += r * u - 1.0;
+            q[2] += r * v;
+            q[3] += en - e_inf;
         }
     }
 }

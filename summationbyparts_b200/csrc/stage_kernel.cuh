@@ -188,6 +188,52 @@ __device__ __forceinline__ void sat_point_rows(double gamma, const double y[4], 
     k[3] += ht * s3;
 }
 
+// sat_point_rows with five reciprocals in place of its divisions and sqrt(kx^2 + ky^2) in place
+// of hypot (no overflow at these magnitudes): the SAT of compensated-f32 systems, still f64, whose
+// last bits need not follow the reference's operation order.
+__device__ __forceinline__ void sat_point_fast(double gamma, const double y[4], const double z[4], double hi,
+                                               double sign, double tau, double detj, double detj_d_dx,
+                                               double detj_d_dy, double igm1, double k[4]) {
+    const double rho = y[0], rhou = y[1], rhov = y[2], e = y[3];
+    const double ij = 1.0 / detj;
+    const double kx_ = detj_d_dx * ij, ky_ = detj_d_dy * ij;
+    const double hyp = sqrt(kx_ * kx_ + ky_ * ky_);
+    const double ih = 1.0 / hyp;
+    const double kx = kx_ * ih, ky = ky_ * ih;
+    const double irho = 1.0 / rho;
+    const double u = rhou * irho, v = rhov * irho;
+    const double gm1 = gamma - 1.0;
+    const double q2 = u * u + v * v;
+    const double p = gm1 * (e - 0.5 * (rhou * u + rhov * v));
+    const double cc = gamma * p * irho;
+    const double c = sqrt(cc);
+    const double icc = 1.0 / cc;
+    const double theta = kx * u + ky * v;
+    const double phi2 = 0.5 * gm1 * q2;
+    const double alpha = 0.70710678118654752440 * rho * c * icc;  // rho / (sqrt(2) c)
+    const double phi2_c2 = (phi2 + cc) * igm1;
+    const double U = kx_ * u + ky_ * v;
+    const double beta = 0.5 * icc;
+    const double r0 = rho - z[0], r1 = rhou - z[1], r2 = rhov - z[2], r3 = e - z[3];
+    const double gc = gm1 * icc;
+    const double t0 = (1.0 - phi2 * icc) * r0 + gc * (u * r1 + v * r2 - r3);
+    const double w = ky * u - kx * v;
+    const double t1 = irho * (-w * r0 + ky * r1 - kx * r2);
+    const double t2 = beta * ((phi2 - c * theta) * r0 + (kx * c - gm1 * u) * r1 + (ky * c - gm1 * v) * r2 + gm1 * r3);
+    const double t3 = beta * ((phi2 + c * theta) * r0 - (kx * c + gm1 * u) * r1 - (ky * c + gm1 * v) * r2 + gm1 * r3);
+    const double L2 = U + c * hyp, L3 = U - c * hyp;
+    const double f0 = U + sign * fabs(U);
+    const double l0 = f0 * t0, l1 = f0 * t1;
+    const double l2 = (L2 + sign * fabs(L2)) * t2;
+    const double l3 = (L3 + sign * fabs(L3)) * t3;
+    const double a2 = alpha * l2, a3 = alpha * l3;
+    const double ht = hi * tau;
+    k[0] += ht * (l0 + a2 + a3);
+    k[1] += ht * (u * l0 + ky * l1 + (u + kx * c) * a2 + (u - kx * c) * a3);
+    k[2] += ht * (v * l0 - kx * l1 + (v + ky * c) * a2 + (v - ky * c) * a3);
+    k[3] += ht * (phi2 * igm1 * l0 + rho * w * l1 + (phi2_c2 + c * theta) * a2 + (phi2_c2 - c * theta) * a3);
+}
+
 // Pointwise quantities of one point (fluxes, euler/src/lib.rs:680-735; upwind_dissipation
 // 619-674) from its state qv and metrics m = (dxi/dx, dxi/dy, deta/dx, deta/dy), each times
 // detJ.  Writes the xi-direction values (Ehat, alpha_u q) and/or eta-direction values (Fhat,
@@ -591,6 +637,8 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
     const int64_t np = B.npad;
     const bool on[4] = {row == ny - 1, row == 0, col == nx - 1, col == 0};
     const double* m64 = A.met64 + B.m_off;
+    // compensated-f32 systems: division-free SAT arithmetic and vortex data (gamma = 1.4)
+    constexpr bool FAST = sizeof(T) == 4;
     const double cst = A.stage == kStageK ? A.ctime : (A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5));
     const double stime = cst == 0.0 ? I.time : I.time + I.dt * cst;
     for (int d = 0; d < 4; ++d) {
@@ -599,7 +647,10 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         const int kind = B.bc_kind[d];
         if (kind == BC_VORTEX) {
             const double* xy = A.xy + B.x_off;
-            vortex_point<true>(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+            if (FAST && A.gamma == 1.4)
+                vortex_point_fast(I, stime, xy[pt], xy[np + pt], zv);
+            else
+                vortex_point<true>(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
         } else if (kind == BC_EVAL) {
             // BoundaryCharacteristic::Eval (euler/src/lib.rs:853-863): the expressions at the stage
             // time, evaluated for this edge point by eval_kernel just before
@@ -664,7 +715,10 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         const double hi = ns ? B.hi_eta : B.hi_xi;
         const double ddx = ns ? m64[3 * np + pt] : m64[np + pt];
         const double ddy = ns ? m64[4 * np + pt] : m64[2 * np + pt];
-        sat_point_rows(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
+        if constexpr (FAST)
+            sat_point_fast(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, I.v_igm1, kv);
+        else
+            sat_point_rows(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
     }
 }
 

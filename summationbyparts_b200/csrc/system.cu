@@ -308,6 +308,17 @@ void set_reference(InstanceDev& I, double gamma) {
     R.c2 = float(gamma * p / rho);
     R.c = float(std::sqrt(gamma * p / rho));
     R.g_rho = float(gamma / rho);
+    // constants of the division-free vortex boundary data (vortex_point_fast)
+    const double PI = 3.14159265358979323846;
+    const double m = I.mach, p_inf = 1.0 / (gamma * m * m);
+    I.v_pinf = p_inf;
+    I.v_igm1 = 1.0 / (gamma - 1.0);
+    for (int k = 0; k < 5; ++k) {
+        const double rs2 = I.rstar[k] * I.rstar[k];
+        I.vk_f[k] = rs2 > 0.0 ? 1.0 / rs2 : 0.0;
+        I.vk_b[k] = rs2 > 0.0 ? I.eps[k] * I.eps[k] * (gamma - 1.0) * m * m / (8.0 * PI * PI * p_inf * rs2) : 0.0;
+        I.vk_u[k] = rs2 > 0.0 ? I.eps[k] / (2.0 * PI * std::sqrt(p_inf) * rs2) : 0.0;
+    }
 }
 
 // Output-pair class tables of the micro-tile kernel (pair_class, stage_kernel_vec.cuh), from the
