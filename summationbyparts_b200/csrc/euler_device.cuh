@@ -16,7 +16,8 @@ namespace sbp {
 enum { BC_THIS = 0, BC_GRID = 1, BC_VORTEX = 2, BC_INTERPOLATE = 3, BC_MULTIGRID = 4, BC_EVAL = 5 };
 enum { NORTH = 0, SOUTH = 1, EAST = 2, WEST = 3 };
 // Device status bits (one word per system, read by the host after steps).  STATUS_BAD_LAUNCH:
-// a stage kernel specialised for one RK stage class was launched for another (a host bug).
+// a stage kernel specialised for one RK stage class was launched for another, or given a tile
+// holding closure outputs of both ends of a line (host bugs).
 enum : unsigned { STATUS_RHO = 1u, STATUS_P = 2u, STATUS_DETJ = 4u, STATUS_NAN = 8u, STATUS_BAD_LAUNCH = 16u };
 
 struct BlockDev {

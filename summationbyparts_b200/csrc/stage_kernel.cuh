@@ -73,7 +73,6 @@ struct StageArgs {
     const float* rinf;       // compensated f32, upwind: free-stream dissipation planes (BlockDev::r_off)
     const double* xy;        // coordinates
     const T* coef;           // operator tables, see coef_base
-    const float4* pair;      // compensated f32: output-pair class tables (pair_row, stage_kernel_vec.cuh)
     double gamma;
     unsigned* status;
 };
@@ -89,14 +88,21 @@ constexpr int kCoefRow = 16;
 constexpr int kCoefStride = (2 * 8 + 1) * kCoefRow;
 __host__ __device__ constexpr int coef_base(int op, int kind) { return (2 * op + kind) * kCoefStride; }
 
-// Extent of the input region of a T-long run of outputs: an interior tile reads H beyond each
-// end; a tile that also holds end-closure rows reads from H before its start to the end of
-// the line, at most M - 1 past its own end (tiles start at multiples of T >= M, so only the
-// first tile can hold start-closure rows, and it reads at most max(T + H, N)).
+// Tiles along a line of n outputs (tile_starts in system.cu) start at multiples of T, except that
+// the last tile starts at e = n - M rounded down to even whenever a multiple of T would fall in
+// (e, n): so the first tile holds every start-closure output, the last every end-closure output,
+// and no tile holds outputs of both ends (n >= 2 M).  The input region of a tile is then at most
+// T + 2 H wide (interior tiles and the first one: H on each side, [0, max(T + H, N)) for the
+// first; the tile before the last ends at e <= n - M, so its region stops H after it), or
+// max(N, M + H + 1) for the last tile, which reads from min(e - H, n - N) to n.
 constexpr int region_extent(int T, int H, int M, int N) {
-    const int a = T + H + (H > M - 1 ? H : M - 1);
-    return a > N ? a : N;
+    const int a = T + 2 * H, b = N > M + H + 1 ? N : M + H + 1;
+    return a > b ? a : b;
 }
+
+// Output rows and columns of a tile: the tile list holds (block, y0, x0, th << 16 | tw).
+__device__ __forceinline__ int tile_rows(const int4& td) { return td.w >> 16; }
+__device__ __forceinline__ int tile_cols(const int4& td) { return td.w & 0xffff; }
 
 // Shared-memory geometry of one tile: xi arrays are TY rows x XP columns, eta arrays HYP rows
 // x 32 columns.
@@ -742,8 +748,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         const int nx = B.nx, ny = B.ny;
         const int64_t np = B.npad;
         const int y0 = td.y, x0 = td.z;
-        const int y1 = min(y0 + TY, ny), x1 = min(x0 + kTileX, nx);
-        const int tw = x1 - x0, th = y1 - y0;
+        const int th = tile_rows(td), tw = tile_cols(td);
+        const int y1 = y0 + th, x1 = x0 + tw;
         int lx0, lx1, ly0, ly1;
         region_of<OPX>(x0, x1, nx, lx0, lx1);
         region_of<OPY>(y0, y1, ny, ly0, ly1);

@@ -18,12 +18,17 @@
 //   128 contiguous bytes of an eta row, or 16 consecutive column slots of the transposed xi
 //   array -- columns 2g + k share k's parity, so the even/odd split puts them in consecutive
 //   slots, and a slot pitch of 17 row pairs (odd) spreads them over all 16 bank pairs: both
-//   kinds of load are conflict-free.  Tiles that hold closure columns run the table path of
-//   stage_kernel for the xi sums on every thread, so warps do not diverge; for the eta sums
-//   only the threads whose row pair holds a closure row take the table path.
+//   kinds of load are conflict-free.
+// * Closures: the first and the last tile of a block row hold all its closure columns (and the
+//   first and last tile of a column all its closure rows; tile_starts in system.cu), and such a
+//   tile first computes the closure outputs' xi (eta) terms with all its threads into a small
+//   shared buffer (closure_xi, closure_eta: the N inputs of the closure block loaded once,
+//   compile-time closure coefficients, first product then an fma chain as the table path of
+//   stage_kernel); every thread then runs the interior path, and the owners of closure outputs
+//   replace its result from the buffer -- no divergence, no per-thread coefficient tables.
 // * The RK operands (1 / J and the stage's state arrays) are read from global memory into
-//   registers one component ahead of their use, which leaves the shared memory of two
-//   256-thread CTAs per SM to the stencil arrays.
+//   registers one component ahead of their use, as 8-byte row pairs, which leaves the shared
+//   memory of two 256-thread CTAs per SM to the stencil arrays.
 #pragma once
 
 #include "stage_kernel.cuh"
@@ -98,81 +103,17 @@ __device__ __forceinline__ void eta_pair(const float* __restrict__ p, float idx,
     out[1] = fmul2s(a1, idx);
 }
 
-// Output pairs with a boundary closure.  A thread's two outputs along a line (columns c0, c0 + 1
-// for xi, rows r0, r0 + 1 for eta; c0 and r0 are even) fall into one of 1.5 M + 2 classes:
-// interior (class 0), both in the start closure (classes 1 .. M/2, by i0 / 2), or near the end
-// (classes M/2 + d for d = n - i0 = 1 .. M + 1: d <= M both in the end closure, or only i0 + 1
-// when d = 1 is past the end; d = M + 1 the first interior and the second in the closure).  For
-// every class the two outputs read inside one window of W consecutive inputs starting at s, and a
-// class's table holds, for each window position k, the pair coefficient (p_k, p_k, q_k, q_k) of
-// output 0 and output 1 (zero where a row has no tap).  So every thread of a closure tile or of a
-// closure row pair runs the same W-tap loop of paired FMAs -- no divergence, no per-tap tests --
-// and only its table row and window start depend on its class.  The coefficients are the f32
-// closure and interior rows of the table path, in the same tap order, so the sums are the same.
-constexpr int kPairW = 14;        // max W over the operators (Upwind9)
-constexpr int kPairClasses = 14;  // max 1.5 M + 2 over the operators
-__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
-__host__ __device__ constexpr int pair_window(int M, int N, int D, int H) { return imax(imax(D + 1, N), M + H + 1); }
-__host__ __device__ constexpr int pair_classes(int M) { return M + M / 2 + 2; }
-
-// Class of the output pair (i0, i0 + 1) of a length-n line (i0 even, i0 < n, n >= 2 M) and the
-// first input s of its window.
-__host__ __device__ __forceinline__ int pair_class(int M, int N, int H, int i0, int n, int& s) {
-    if (i0 < M) {
-        s = 0;
-        return 1 + i0 / 2;
-    }
-    const int d = n - i0;
-    if (d <= M + 1) {
-        s = d == M + 1 ? (i0 - H < n - N ? i0 - H : n - N) : n - N;
-        return M / 2 + d;
-    }
-    s = i0 - H;
-    return 0;
-}
-template <int OP>
-__device__ __forceinline__ int pair_class(int i0, int n, int& s) {
-    return pair_class(OpShape<OP>::M, OpShape<OP>::N, OpShape<OP>::H, i0, n, s);
-}
-template <int OP>
-__device__ __forceinline__ bool closure_pair(int i0, int n) {
-    return i0 < OpShape<OP>::M || i0 + 1 >= n - OpShape<OP>::M;
-}
-
-// Sums of one kind for an output pair of any class: ld(k) is the input pair at window position
-// k, cf the class's table row (W entries).
-template <int OP, class LD>
-__device__ __forceinline__ void pair_sums(const LD& ld, const float4* __restrict__ cf, float idx, float2 out[2]) {
-    constexpr int W = pair_window(OpShape<OP>::M, OpShape<OP>::N, OpShape<OP>::D, OpShape<OP>::H);
-    float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-        const float2 v = ld(k);
-        const float4 c = __ldg(cf + k);
-        a0 = __ffma2_rn(v, make_float2(c.x, c.y), a0);
-        a1 = __ffma2_rn(v, make_float2(c.z, c.w), a1);
-    }
-    out[0] = fmul2s(a0, idx);
-    out[1] = fmul2s(a1, idx);
-}
-
-// Table row of class `cls` for operator op and kind (DIFF, DISS) in the pair table.
-__device__ __forceinline__ const float4* pair_row(const float4* pair, int op, int kind, int cls) {
-    return pair + ((2 * op + kind) * kPairClasses + cls) * kPairW;
-}
-
-// Closure terms of a tile: xi ([component][closure column][row], row pitch 34, closure_xi) or
-// eta ([component][closure row][column], closure_eta), one at a time.
+// Closure terms of a tile: xi ([component][closure column][row], row pitch 34, closure_xi) and
+// eta ([component][closure row][column], closure_eta), one buffer each.
 constexpr int kClosurePitch = 34;
-__host__ __device__ constexpr int closure_buffer_elems(int mx, int my) {
-    return 4 * mx * kClosurePitch > 4 * my * kTileX ? 4 * mx * kClosurePitch : 4 * my * kTileX;
-}
-
+__host__ __device__ constexpr int closure_xi_elems(int mx) { return 4 * mx * kClosurePitch; }
+__host__ __device__ constexpr int closure_eta_elems(int my) { return 4 * my * kTileX; }
 
 template <int OPX, int OPY>
 constexpr size_t vec_stage_smem(bool upw) {
     using G = VecGeom<OPX, OPY>;
-    return sizeof(float) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + closure_buffer_elems(OpShape<OPX>::M, OpShape<OPY>::M));
+    return sizeof(float) * ((size_t)(4 * G::XA + 4 * G::YA) * (upw ? 2 : 1) + closure_xi_elems(OpShape<OPX>::M) +
+                            closure_eta_elems(OpShape<OPY>::M));
 }
 
 // Closure-block coefficient (row I, input K) of one end of a line: the start block, or the end
@@ -264,7 +205,6 @@ template <int OPX, int OPY, bool UPW, int SC>
 __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const StageArgs<float> A) {
     static_assert(SC >= 0 && SC <= 2, "stage class");
     using G = VecGeom<OPX, OPY>;
-    constexpr int TY = kVecRows;
     constexpr int XA = G::XA, YA = G::YA, XCH = G::XCH;
     constexpr int HX = OpShape<OPX>::H, HY = OpShape<OPY>::H;
     // phase-1 points per thread and batch: enough for an interior tile's whole region
@@ -273,7 +213,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sE = reinterpret_cast<float*>(smem_raw);  // [UPW ? 8 : 4][2 XCH][34]: Ehat, alpha_u q (transposed)
     float* sF = sE + (UPW ? 8 : 4) * XA;             // [UPW ? 8 : 4][HYP][32]: Fhat, alpha_v q
-    float* cbuf = sF + (UPW ? 8 : 4) * YA;           // closure terms (closure_buffer_elems)
+    float* cbuf = sF + (UPW ? 8 : 4) * YA;           // [4][M_xi][34]: closure-column xi terms
+    float* cbuf_y = cbuf + closure_xi_elems(OpShape<OPX>::M);  // [4][M_eta][32]: closure-row eta terms
     const float gamma = float(A.gamma);
     const int tid = threadIdx.x;
     const int grp = tid & 15, rpr = tid >> 4;  // column pair, row pair (0..15 each)
@@ -281,14 +222,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
     if (A.stage == kStageK || vec_stage_class(A.stage) != SC) {  // launched for another stage class
         if (tid == 0) atomicOr(A.status, STATUS_BAD_LAUNCH);
         return;
-    }
-    // Every shared array starts at zero: a pair-class window may reach slots that no tile of this
-    // CTA has written (their coefficients are zero), and those must hold finite values.
-    {
-        float4* z = reinterpret_cast<float4*>(smem_raw);
-        constexpr int n4 = (int)(vec_stage_smem<OPX, OPY>(UPW) / sizeof(float4));
-        for (int i = tid; i < n4; i += kStageThreads) z[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        __syncthreads();
     }
     // RK operand arrays (stage_operands): stage 0 u_in; stages 1, 2 acc_hi, prev_hi; stage 3 also prev_lo
     constexpr int NSRC = SC + 1;
@@ -300,8 +233,8 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const int nx = B.nx, ny = B.ny;
         const int np = (int)B.npad;  // in-block offsets fit 32 bits (checked when the system is built)
         const int y0 = td.y, x0 = td.z;
-        const int y1 = min(y0 + TY, ny), x1 = min(x0 + kTileX, nx);
-        const int tw = x1 - x0, th = y1 - y0;
+        const int th = tile_rows(td), tw = tile_cols(td);
+        const int y1 = y0 + th, x1 = x0 + tw;
         int lx0, lx1, ly0, ly1;
         region_of<OPX>(x0, x1, nx, lx0, lx1);
         region_of<OPY>(y0, y1, ny, ly0, ly1);
@@ -408,13 +341,20 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         }
         __syncthreads();
 
-        // A tile holding the closure columns of one end of its rows: their xi sums for every row
-        // and array go to cbuf first (all threads, one barrier) and replace, in phase 2, what the
-        // interior path computes for those columns.  A tile holding both ends (rows shorter than
-        // a tile and a half) takes the pair-class path instead.
+        // Closure outputs.  The tile list gives every closure column of a block row to its first
+        // or its last tile and no tile both (tile_starts), and likewise for rows.  A tile holding
+        // closure columns first writes their xi terms (diss - diff, scaled) for every row and
+        // component into cbuf, a tile holding closure rows their eta terms into cbuf_y (all
+        // threads, one barrier for both); in phase 2 every thread runs the interior path and the
+        // threads owning closure outputs replace its result from the buffers.
         const bool left_cl = x0 < OpShape<OPX>::M, right_cl = x1 > nx - OpShape<OPX>::M;
-        const bool one_end = left_cl != right_cl;
-        if (one_end) {
+        const bool top_cl = y0 < OpShape<OPY>::M, bot_cl = y1 > ny - OpShape<OPY>::M;
+        if ((left_cl && right_cl) || (top_cl && bot_cl)) {  // a tile list not made by tile_starts
+            if (tid == 0) atomicOr(A.status, STATUS_BAD_LAUNCH);
+            return;
+        }
+        const bool xi_pre = left_cl || right_cl, eta_pre = top_cl || bot_cl;
+        if (xi_pre) {
             // thread: component tid / 64, tile row (tid / 2) % 32, half tid % 2 of the M columns
             constexpr int MX = OpShape<OPX>::M;
             const int comp = tid >> 6, r = (tid >> 1) & 31, half = tid & 1;
@@ -431,21 +371,16 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     else closure_xi<OPX, UPW, false, XCH, 0, MX / 2>(e, al, lc, idxx, cb);
                 }
             }
-            __syncthreads();
         }
-        // The same for a tile holding the closure rows of one end of its columns when the buffer
-        // is free (no xi closure): thread = component tid / 64, half (tid / 32) % 2 of the M rows,
-        // tile column tid % 32.  Other tiles with closure rows take the pair-class path.
-        const bool top_cl = y0 < OpShape<OPY>::M, bot_cl = y1 > ny - OpShape<OPY>::M;
-        const bool eta_pre = top_cl != bot_cl && !one_end;
         if (eta_pre) {
+            // thread: component tid / 64, half (tid / 32) % 2 of the M rows, tile column tid % 32
             constexpr int MY = OpShape<OPY>::M;
             const int comp = tid >> 6, half = (tid >> 5) & 1, col = tid & 31;
             if (col < tw) {
                 const int lr = bot_cl ? ny - OpShape<OPY>::N - ly0 : -ly0;
                 const float* f = sF + comp * YA + col;
                 const float* al = sF + (UPW ? 4 + comp : comp) * YA + col;
-                float* cb = cbuf + comp * MY * kTileX + col;
+                float* cb = cbuf_y + comp * MY * kTileX + col;
                 if (bot_cl) {
                     if (half) closure_eta<OPY, UPW, true, MY / 2, MY / 2>(f, al, lr, idxy, cb);
                     else closure_eta<OPY, UPW, true, 0, MY / 2>(f, al, lr, idxy, cb);
@@ -454,19 +389,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                     else closure_eta<OPY, UPW, false, 0, MY / 2>(f, al, lr, idxy, cb);
                 }
             }
-            __syncthreads();
         }
+        if (xi_pre || eta_pre) __syncthreads();
 
         // ---------------- phase 2: stencils and stage update ----------------
         if (active) {
-            // xi: tiles holding both ends' closure columns run the pair-class path on every thread
-            // (the class follows the thread's column pair); eta: warps holding a closure row pair
-            // (warp w has row pairs 2 w, 2 w + 1) run it with each thread's own class
-            // (warp-uniform choice)
-            const bool xi_closure = left_cl && right_cl;
-            const int wr = y0 + 4 * (tid >> 5);  // first row of the warp
-            const bool eta_closure =
-                !eta_pre && (closure_pair<OPY>(wr, ny) || (wr + 2 < ny && closure_pair<OPY>(wr + 2, ny)));
             const float* xrow = sE + (r0 - y0);                                  // xi arrays at row r0
             // interior-path window from column c0 - H (kept inside the arrays for closure columns,
             // whose interior-path sums are replaced)
@@ -483,23 +410,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
 #pragma unroll
                 for (int j = 0; j < 2; ++j)
                     edge[u][j] = r0 + u == 0 || r0 + u == ny - 1 || c0 + j == 0 || c0 + j == nx - 1;
-            // pair-class windows and table rows (closure tiles and warps only)
-            const float *gxe = xwe, *gxo = xwo, *gy = ewin;
-            const float4 *cfx = nullptr, *cfy = nullptr;
-            if (xi_closure) {
-                int sx;
-                const int cls = pair_class<OPX>(c0, nx, sx);
-                gxe = xrow + xslot<XCH>(sx - lx0) * kVecPitch;
-                gxo = xrow + xslot<XCH>(sx - lx0 + 1) * kVecPitch;
-                cfx = pair_row(A.pair, OPX, DIFF, cls);
-            }
-            if (eta_closure) {
-                int sy;
-                const int cls = pair_class<OPY>(r0, ny, sy);
-                gy = ecol + (sy - ly0) * kTileX;
-                cfy = pair_row(A.pair, OPY, DIFF, cls);
-            }
-            constexpr int kDissRow = kPairClasses * kPairW;  // DISS rows follow the DIFF rows of an operator
             // outputs: stage 3 the new (hi, lo) state, otherwise the next stage input and the increment
             // per-array pointers at point (r0, c0) of component cc, advanced by one plane per
             // component: the four points are at offsets 0, 1, nx, nx + 1
@@ -526,41 +436,12 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
                 float2 ey[2], ay[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
-                if (!xi_closure && !eta_closure) {
-                    xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
-                    if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
-                    eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
-                    if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
-                } else {
-                    if (!xi_closure) {
-                        xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
-                        if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
-                    } else {
-                        // window position k = column sx + k: slots alternate between the two parities
-                        const float *pe = gxe + cc * XA, *po = gxo + cc * XA;
-                        pair_sums<OPX>([&](int k) { return *reinterpret_cast<const float2*>((k & 1 ? po : pe) + (k >> 1) * kVecPitch); },
-                                       cfx, idxx, ex);
-                        if constexpr (UPW) {
-                            const float *qe = pe + 4 * XA, *qo = po + 4 * XA;
-                            pair_sums<OPX>([&](int k) { return *reinterpret_cast<const float2*>((k & 1 ? qo : qe) + (k >> 1) * kVecPitch); },
-                                           cfx + kDissRow, idxx, dx);
-                        }
-                    }
-                    // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
-                    if (!eta_closure) {
-                        eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
-                        if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
-                    } else {
-                        const float* pw = gy + cc * YA;
-                        pair_sums<OPY>([&](int k) { return *reinterpret_cast<const float2*>(pw + k * kTileX); }, cfy, idxy, ey);
-                        if constexpr (UPW) {
-                            const float* qw = pw + 4 * YA;
-                            pair_sums<OPY>([&](int k) { return *reinterpret_cast<const float2*>(qw + k * kTileX); }, cfy + kDissRow,
-                                           idxy, ay);
-                        }
-                    }
-                }
-                if (one_end) {
+                xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
+                if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
+                // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
+                eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
+                if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
+                if (xi_pre) {
 #pragma unroll
                     for (int j = 0; j < 2; ++j) {
                         const int ci = left_cl ? c0 + j : c0 + j - (nx - OpShape<OPX>::M);
@@ -579,7 +460,7 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                         const int ri = top_cl ? r0 + u : r0 + u - (ny - OpShape<OPY>::M);
                         if (ri >= 0 && ri < OpShape<OPY>::M && rok[u]) {
                             const float2 t = *reinterpret_cast<const float2*>(
-                                cbuf + (cc * OpShape<OPY>::M + ri) * kTileX + (c0 - x0));
+                                cbuf_y + (cc * OpShape<OPY>::M + ri) * kTileX + (c0 - x0));
                             ey[u] = make_float2(-t.x, -t.y);
                             ay[u] = make_float2(0.0f, 0.0f);
                         }

@@ -75,7 +75,8 @@ size_t stage_smem_host(int prec, int opx, int opy, bool upw, int ty) {
         const int xc = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
         const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
         return sizeof(float) *
-               ((size_t)(4 * 2 * ((xc + 1) / 2) * kVecPitch + 4 * hyp * kTileX) * (upw ? 2 : 1) + closure_buffer_elems(ox.M, oy.M));
+               ((size_t)(4 * 2 * ((xc + 1) / 2) * kVecPitch + 4 * hyp * kTileX) * (upw ? 2 : 1) + closure_xi_elems(ox.M) +
+                closure_eta_elems(oy.M));
     }
     const int xp = region_extent(kTileX, (ox.D - 1) / 2, ox.M, ox.N);
     const int hyp = region_extent(ty, (oy.D - 1) / 2, oy.M, oy.N);
@@ -161,7 +162,6 @@ struct sbp_system {
     double* d_sums = nullptr;
     unsigned long long* d_speeds = nullptr;
     void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
-    float4* d_pair = nullptr;  // compensated f32: output-pair class tables of the micro-tile kernel
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
@@ -232,7 +232,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf,    s->d_pair};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -321,53 +321,6 @@ void set_reference(InstanceDev& I, double gamma) {
     }
 }
 
-// Output-pair class tables of the micro-tile kernel (pair_class, stage_kernel_vec.cuh), from the
-// f32 coefficient table `coef` (layout of coef_base): for every operator, kind and class, the W
-// window positions' (p, p, q, q), p the coefficient output 0 of the pair applies to the input at
-// that position and q output 1's, zero where the output's row has no tap.
-constexpr int kPairTableEntries = 12 * kPairClasses * kPairW;
-bool pair_table(const float* coef, std::vector<float4>& out) {
-    out.assign(kPairTableEntries, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
-    for (int op = 0; op < 6; ++op) {
-        OpInfo oi;
-        op_info(op, oi);
-        const int M = oi.M, N = oi.N, D = oi.D, H = (D - 1) / 2;
-        const int W = pair_window(M, N, D, H), ncls = pair_classes(M);
-        const int n = 1000;  // any line long enough: the classes depend on positions relative to its ends
-        // table row, first input and tap count of output i (table_row of the table path)
-        auto row_of = [&](int i, int& row, int& base, int& ntaps) {
-            if (i < M) {
-                row = i, base = 0, ntaps = N;
-            } else if (i >= n - M) {
-                row = M + i - (n - M), base = n - N, ntaps = N;
-            } else {
-                row = 2 * M, base = i - H, ntaps = D;
-            }
-        };
-        for (int cls = 0; cls < ncls; ++cls) {
-            const int i0 = cls == 0 ? 100 : (cls <= M / 2 ? 2 * (cls - 1) : n - (cls - M / 2));
-            int s0 = 0;
-            if (pair_class(M, N, H, i0, n, s0) != cls) return false;  // the class numbering above
-            for (int kind = 0; kind < (oi.upwind ? 2 : 1); ++kind) {
-                const float* tab = coef + (2 * op + kind) * kCoefStride;
-                float4* dst = out.data() + ((2 * op + kind) * kPairClasses + cls) * kPairW;
-                for (int o = 0; o < 2 && i0 + o < n; ++o) {
-                    int row, base, ntaps;
-                    row_of(i0 + o, row, base, ntaps);
-                    for (int t = 0; t < ntaps; ++t) {
-                        const int k = base + t - s0;
-                        if (k < 0 || k >= W) return false;  // the window covers every tap
-                        const float c = tab[row * kCoefRow + t];
-                        if (o == 0) dst[k].x = dst[k].y = c;
-                        else dst[k].z = dst[k].w = c;
-                    }
-                }
-            }
-        }
-    }
-    return true;
-}
-
 template <class T>
 StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     StageArgs<T> a{};
@@ -393,7 +346,6 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.rinf = s->rinf;
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
-    a.pair = s->d_pair;
     a.kedge = static_cast<T*>(s->kedge);
     a.mg = s->d_mg;
     a.eval = s->d_eval;
@@ -529,6 +481,25 @@ const Tableau* tableau_of(int id) {
 // Build per-operator-pair tile lists for the blocks of the instances flagged in `active`, size
 // shared memory and grids, and capture one RK4 step (time update with the device mask
 // d_active) into a graph.
+// Tile boundaries along a line of n >= 2 M outputs, tiles of up to T, for an operator with M
+// closure rows: multiples of T, except that the boundaries in (e, n), e = n - M rounded down to
+// even, give way to e (and a line shorter than T + M is cut at e), so the last tile holds every
+// end-closure output and no tile holds outputs of both ends (region_extent in stage_kernel.cuh).
+// Returns the starts followed by n.
+std::vector<int> tile_starts(int n, int T, int M) {
+    std::vector<int> b;
+    const int e = (n - M) & ~1;
+    bool moved = false;
+    for (int x = 0; x < n; x += T) {
+        if (x <= e) b.push_back(x);
+        else moved = true;
+    }
+    // a boundary was dropped, or the last tile would also hold start-closure outputs
+    if ((moved || b.back() < M) && b.back() != e) b.push_back(e);
+    b.push_back(n);
+    return b;
+}
+
 sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const int* d_active,
                             std::vector<Group>& groups, cudaGraph_t& graph_out, cudaGraphExec_t& gexec_out) {
     free_group_list(groups, graph_out, gexec_out);
@@ -576,14 +547,16 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             if (groups[gi].opx == B.op_xi && groups[gi].opy == B.op_eta && groups[gi].upw == upw) break;
         Group& g = groups[gi];
         const int TY = g.ty;
-        for (int y0 = 0; y0 < B.ny; y0 += TY)
-            for (int x0 = 0; x0 < B.nx; x0 += TX) {
+        const std::vector<int> ys = tile_starts(B.ny, TY, oy.M), xs = tile_starts(B.nx, TX, ox.M);
+        for (size_t iy = 0; iy + 1 < ys.size(); ++iy)
+            for (size_t ix = 0; ix + 1 < xs.size(); ++ix) {
+                const int y0 = ys[iy], y1 = ys[iy + 1], x0 = xs[ix], x1 = xs[ix + 1];
                 int lo, hi;
-                region_host(B.op_xi, x0, std::min(x0 + TX, B.nx), B.nx, lo, hi);
+                region_host(B.op_xi, x0, x1, B.nx, lo, hi);
                 g.WX = std::max(g.WX, hi - lo);
-                region_host(B.op_eta, y0, std::min(y0 + TY, B.ny), B.ny, lo, hi);
+                region_host(B.op_eta, y0, y1, B.ny, lo, hi);
                 g.HY = std::max(g.HY, hi - lo);
-                tiles[gi].push_back(make_int4(b, y0, x0, 0));
+                tiles[gi].push_back(make_int4(b, y0, x0, (y1 - y0) << 16 | (x1 - x0)));
             }
         g.points += (int64_t)B.nx * B.ny;
         // edge points in edge_index order: first row, last row, first column, last column
@@ -1049,7 +1022,6 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_sums, (size_t)nblocks * (1 + kNormParts) * sizeof(double));
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
-    if (s->prec == 1) e = e ?: alloc((void**)&s->d_pair, kPairTableEntries * sizeof(float4));
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
     e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
     e = e ?: alloc((void**)&s->d_eval, sizeof(EvalDev));
@@ -1071,15 +1043,6 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     std::vector<double> coef_host(12 * kCoefStride);  // large enough for either precision
     fill_coef_table(s->prec, coef_host.data(), kCoefStride, kCoefRow);
     e = e ?: cudaMemcpyAsync(s->d_coef, coef_host.data(), 12 * kCoefStride * ts, cudaMemcpyHostToDevice, st);
-    std::vector<float4> pair_host;
-    if (s->prec == 1) {
-        if (!pair_table(reinterpret_cast<const float*>(coef_host.data()), pair_host)) {
-            set_error("internal: output-pair class table does not cover the operators' taps");
-            return fail(SBP_ERR_INVALID_ARGUMENT);
-        }
-        e = e ?: cudaMemcpyAsync(s->d_pair, pair_host.data(), kPairTableEntries * sizeof(float4), cudaMemcpyHostToDevice,
-                                 st);
-    }
     {
         std::vector<int64_t> p8(nblocks);
         for (int b = 0; b < nblocks; ++b) p8[b] = 2 * s->dense_off[b];
