@@ -65,6 +65,7 @@ struct StageArgs {
     T* new_hi;               // new state (stage 3)
     T* new_lo;
     T* kedge;                // k of block-edge points, 4 per point (edge_index order per block)
+    const double* egeo;      // compensated f32: edge geometry, kEdgeGeo per point (edge_geo_kernel)
     const int4* mg;          // MultiGrid segments (block, start, end, -) of all block sides
     const EvalDev* eval;     // expression programs of SBP_BC_EVAL sides
     double* evz;             // SBP_BC_EVAL data of the launch's edge points (eval_kernel), 4 per point
@@ -635,14 +636,35 @@ __device__ __forceinline__ double absolute_state(const StageArgs<T>& A, const Bl
     else return double(v);
 }
 
+// The time-independent data of one block-edge point the SATs read: coordinates, the f64
+// metrics (detJ, J dxi/dx, J dxi/dy, J deta/dx, J deta/dy).
+struct EdgeGeo {
+    double x, y, m[5];
+};
+// Compensated-f32 systems gather the geometry of their block-edge points once into one contiguous
+// 64-byte record per point (slot e_off + edge_index: x, y, detJ, the 4 metric terms, padding;
+// edge_geo_kernel), which the edge kernel reads instead of seven scattered sectors (the first and
+// last columns of a block are nx elements apart).
+constexpr int kEdgeGeo = 8;
+template <class T>
+__device__ __forceinline__ EdgeGeo edge_geo(const StageArgs<T>& A, const BlockDev& B, int pt) {
+    const int64_t np = B.npad;
+    const double* m64 = A.met64 + B.m_off;
+    const double* xy = A.xy + B.x_off;
+    EdgeGeo g;
+    g.x = xy[pt];
+    g.y = xy[np + pt];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) g.m[c] = m64[c * np + pt];
+    return g;
+}
+
 // SATs of one block-edge point in the reference's order N, S, E, W; k updated in place.
 template <class T>
 __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDev& I, const BlockDev& B, int eidx, int row,
-                                      int col, int pt, const double yv[4], double kv[4]) {
+                                      int col, const EdgeGeo& geo, const double yv[4], double kv[4]) {
     const int nx = B.nx, ny = B.ny;
-    const int64_t np = B.npad;
     const bool on[4] = {row == ny - 1, row == 0, col == nx - 1, col == 0};
-    const double* m64 = A.met64 + B.m_off;
     // compensated-f32 systems: division-free SAT arithmetic and vortex data (gamma = 1.4)
     constexpr bool FAST = sizeof(T) == 4;
     const double cst = A.stage == kStageK ? A.ctime : (A.stage == 0 ? 0.0 : (A.stage == 3 ? 1.0 : 0.5));
@@ -652,11 +674,10 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         double zv[4];
         const int kind = B.bc_kind[d];
         if (kind == BC_VORTEX) {
-            const double* xy = A.xy + B.x_off;
             if (FAST && A.gamma == 1.4)
-                vortex_point_fast(I, stime, xy[pt], xy[np + pt], zv);
+                vortex_point_fast(I, stime, geo.x, geo.y, zv);
             else
-                vortex_point<true>(I, A.gamma, stime, xy[pt], xy[np + pt], zv);
+                vortex_point<true>(I, A.gamma, stime, geo.x, geo.y, zv);
         } else if (kind == BC_EVAL) {
             // BoundaryCharacteristic::Eval (euler/src/lib.rs:853-863): the expressions at the stage
             // time, evaluated for this edge point by eval_kernel just before
@@ -719,12 +740,12 @@ __device__ __forceinline__ void sat_edge(const StageArgs<T>& A, const InstanceDe
         const double sign = (d == NORTH || d == EAST) ? -1.0 : 1.0;
         const double tau = (d == NORTH || d == EAST) ? 1.0 : -1.0;
         const double hi = ns ? B.hi_eta : B.hi_xi;
-        const double ddx = ns ? m64[3 * np + pt] : m64[np + pt];
-        const double ddy = ns ? m64[4 * np + pt] : m64[2 * np + pt];
+        const double ddx = ns ? geo.m[3] : geo.m[1];
+        const double ddy = ns ? geo.m[4] : geo.m[2];
         if constexpr (FAST)
-            sat_point_fast(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, I.v_igm1, kv);
+            sat_point_fast(A.gamma, yv, zv, hi, sign, tau, geo.m[0], ddx, ddy, I.v_igm1, kv);
         else
-            sat_point_rows(A.gamma, yv, zv, hi, sign, tau, m64[pt], ddx, ddy, kv);
+            sat_point_rows(A.gamma, yv, zv, hi, sign, tau, geo.m[0], ddx, ddy, kv);
     }
 }
 
@@ -944,9 +965,39 @@ __global__ void __launch_bounds__(kSatThreads, 4) sat_kernel(const StageArgs<T> 
         yv[cc] = absolute_state<T>(A, B, cc, qs[cc]);
         kv[cc] = double(A.kedge[slot + cc]);
     }
-    sat_edge<T>(A, I, B, i, row, col, pt, yv, kv);
+    EdgeGeo geo;
+    if (sizeof(T) == 4 && A.egeo) {
+        const double2* gp = reinterpret_cast<const double2*>(A.egeo + kEdgeGeo * (B.e_off + edge_index(row, col, nx, ny)));
+        const double2 g0 = gp[0], g1 = gp[1], g2 = gp[2], g3 = gp[3];
+        geo.x = g0.x;
+        geo.y = g0.y;
+        geo.m[0] = g1.x;
+        geo.m[1] = g1.y;
+        geo.m[2] = g2.x;
+        geo.m[3] = g2.y;
+        geo.m[4] = g3.x;
+    } else {
+        geo = edge_geo(A, B, pt);
+    }
+    sat_edge<T>(A, I, B, i, row, col, geo, yv, kv);
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) rk_update<T, COMP>(A, qoff + cc * np + pt, qs[cc], T(kv[cc]), cb, ca);
+}
+
+// Edge geometry of a group's edge points (edges[i] = block, row, col) at their slots.
+template <class T>
+__global__ void edge_geo_kernel(const StageArgs<T> A, const int4* __restrict__ edges, int nedges, double* __restrict__ geo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nedges) return;
+    const int4 ed = edges[i];
+    const BlockDev& B = A.blocks[ed.x];
+    const EdgeGeo g = edge_geo(A, B, ed.y * B.nx + ed.z);
+    double* o = geo + kEdgeGeo * (B.e_off + edge_index(ed.y, ed.z, B.nx, B.ny));
+    o[0] = g.x;
+    o[1] = g.y;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) o[2 + c] = g.m[c];
+    o[7] = 0.0;
 }
 
 // Expression boundary data (SBP_BC_EVAL sides) of a stage launch's edge points (edges[i] =

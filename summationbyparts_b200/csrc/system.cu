@@ -163,6 +163,7 @@ struct sbp_system {
     unsigned long long* d_speeds = nullptr;
     void* d_coef = nullptr;  // stage-kernel coefficient table in the state precision
     void* kedge = nullptr;   // k of block-edge points between the stage and the edge kernel
+    double* egeo = nullptr;   // compensated f32: edge geometry (kEdgeGeo per point, edge_geo_kernel)
     int64_t nedge = 0;
     int4* d_mg = nullptr;    // MultiGrid segments of all block sides
     EvalDev* d_eval = nullptr;  // expression programs of SBP_BC_EVAL sides
@@ -232,7 +233,7 @@ void destroy_all(sbp_system* s) {
     void* ptrs[] = {s->d_blocks, s->d_inst, s->d_active, s->prev_hi, s->prev_lo, s->acc_hi, s->acc_lo,
                     s->uA,       s->uB,     s->met64,    s->met32,   s->xy,      s->hw,      s->d_hoff,
                     s->d_poff4,  s->d_poff8, s->d_zero,  s->staging, s->status,  s->d_sums,  s->d_speeds,
-                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf};
+                    s->d_coef,   s->kedge,  s->d_mg,     s->kbuf,    s->d_eval,  s->rinf,    s->egeo};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto st : s->side) cudaStreamDestroy(st);
@@ -347,6 +348,7 @@ StageArgs<T> stage_args(sbp_system* s, int stage, const Group& g) {
     a.xy = s->xy;
     a.coef = static_cast<const T*>(s->d_coef);
     a.kedge = static_cast<T*>(s->kedge);
+    a.egeo = s->egeo;
     a.mg = s->d_mg;
     a.eval = s->d_eval;
     a.evz = g.d_evz;
@@ -609,6 +611,12 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
             SBP_TRY_CUDA(cudaMemcpyAsync(g.d_edges, edges[gi].data(), g.nedges * sizeof(int4),
                                          cudaMemcpyHostToDevice, s->stream));
             if (s->has_eval) SBP_TRY_CUDA(cudaMalloc(&g.d_evz, (size_t)g.nedges * 4 * sizeof(double)));
+            if (s->prec == 1) {
+                // the geometry of the group's edge points for the edge kernel (time-independent)
+                StageArgs<float> a = stage_args<float>(s, 0, g);
+                edge_geo_kernel<float><<<(g.nedges + 127) / 128, 128, 0, s->stream>>>(a, g.d_edges, g.nedges, s->egeo);
+                SBP_TRY_CUDA(cudaGetLastError());
+            }
         }
     }
     SBP_TRY_CUDA(cudaStreamSynchronize(s->stream));
@@ -1023,6 +1031,9 @@ sbp_status sbp_system_create(int device, const sbp_block_desc* blocks, int nbloc
     e = e ?: alloc((void**)&s->d_speeds, 2 * nblocks * sizeof(unsigned long long));
     e = e ?: alloc(&s->d_coef, 12 * kCoefStride * ts);
     e = e ?: alloc(&s->kedge, 4 * s->nedge * ts);
+    if (s->prec == 1) {
+        e = e ?: alloc((void**)&s->egeo, kEdgeGeo * s->nedge * sizeof(double));
+    }
     e = e ?: alloc((void**)&s->d_mg, (mg_host.size() + 1) * sizeof(int4));
     e = e ?: alloc((void**)&s->d_eval, sizeof(EvalDev));
     if (e != cudaSuccess) return fail(cuda_status(e, "device allocation"));
