@@ -880,8 +880,9 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel(const StageArgs
         const int nrows = min(R, y1 - r0);
         if (lane < tw && nrows > 0) {
             const int col = x0 + lane;
-            const T idxx = sizeof(T) == 8 ? T(B.idx_xi) : T(B.idx_xi_f);
-            const T idxy = sizeof(T) == 8 ? T(B.idx_eta) : T(B.idx_eta_f);
+            // the compensated form's f32 metrics carry the spacing factors already
+            const T idxx = COMP ? T(1) : (sizeof(T) == 8 ? T(B.idx_xi) : T(B.idx_xi_f));
+            const T idxy = COMP ? T(1) : (sizeof(T) == 8 ? T(B.idx_eta) : T(B.idx_eta_f));
             const bool fused = col < (sizeof(T) == 8 ? B.simd_f64 : B.simd_f32);
             const bool eta_interior = r0 >= OpShape<OPY>::M && r0 + R <= ny - OpShape<OPY>::M;
             const bool edge_col = col == 0 || col == nx - 1;

@@ -52,7 +52,6 @@ template <int XCH>
 __device__ __forceinline__ int xslot(int c) { return (c >> 1) + (c & 1) * XCH; }
 
 __device__ __forceinline__ float2 ffma2(float2 a, float c, float2 acc) { return __ffma2_rn(a, make_float2(c, c), acc); }
-__device__ __forceinline__ float2 fmul2s(float2 a, float c) { return __fmul2_rn(a, make_float2(c, c)); }
 
 // Taps I..D of two adjacent outputs of one stencil: ld(i) is the input pair at tap position i of
 // the first output (D + 1 positions for the two); output 0 takes coefficient i at position i,
@@ -82,25 +81,24 @@ struct PairTaps {
 // (pe, po: the slots of columns c0 - H and c0 - H + 1; 8-byte aligned).  Interior columns: the
 // fma chain of stage_kernel's interior path (its zero taps skipped).
 template <int OP, int KIND>
-__device__ __forceinline__ void xi_pair(const float* __restrict__ pe, const float* __restrict__ po, float idx,
-                                        float2 out[2]) {
+__device__ __forceinline__ void xi_pair(const float* __restrict__ pe, const float* __restrict__ po, float2 out[2]) {
     constexpr int D = OpShape<OP>::D;
     float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
     PairTaps<OP, KIND, 0, D>::run(
         [&](int i) { return *reinterpret_cast<const float2*>((i & 1 ? po : pe) + (i >> 1) * kVecPitch); }, a0, a1);
-    out[0] = fmul2s(a0, idx);
-    out[1] = fmul2s(a1, idx);
+    out[0] = a0;
+    out[1] = a1;
 }
 
 // Eta sums of one kind at rows r0, r0 + 1, each over the thread's two columns: p points at the
 // eta array's row r0 - H, column c0 (8-byte aligned).
 template <int OP, int KIND>
-__device__ __forceinline__ void eta_pair(const float* __restrict__ p, float idx, float2 out[2]) {
+__device__ __forceinline__ void eta_pair(const float* __restrict__ p, float2 out[2]) {
     constexpr int D = OpShape<OP>::D;
     float2 a0 = make_float2(0.0f, 0.0f), a1 = make_float2(0.0f, 0.0f);
     PairTaps<OP, KIND, 0, D>::run([&](int i) { return *reinterpret_cast<const float2*>(p + i * kTileX); }, a0, a1);
-    out[0] = fmul2s(a0, idx);
-    out[1] = fmul2s(a1, idx);
+    out[0] = a0;
+    out[1] = a1;
 }
 
 // Closure terms of a tile: xi ([component][closure column][row], row pitch 34, closure_xi) and
@@ -139,21 +137,21 @@ __device__ __forceinline__ float closure_sum(const float* v, float t) {
 
 // Writes closure columns I .. I + CNT - 1 of closure_xi.
 template <int OP, bool UPW, bool RIGHT, int I, int CNT, int PITCH = kClosurePitch>
-__device__ __forceinline__ void closure_out(const float* ve, const float* va, float idx, float* cb) {
+__device__ __forceinline__ void closure_out(const float* ve, const float* va, float* cb) {
     if constexpr (CNT > 0) {
         float d = 0.0f;
-        if constexpr (UPW) d = closure_sum<OP, DISS, RIGHT, I>(va, 0.0f) * idx;
-        cb[I * PITCH] = d - closure_sum<OP, DIFF, RIGHT, I>(ve, 0.0f) * idx;
-        closure_out<OP, UPW, RIGHT, I + 1, CNT - 1, PITCH>(ve, va, idx, cb);
+        if constexpr (UPW) d = closure_sum<OP, DISS, RIGHT, I>(va, 0.0f);
+        cb[I * PITCH] = d - closure_sum<OP, DIFF, RIGHT, I>(ve, 0.0f);
+        closure_out<OP, UPW, RIGHT, I + 1, CNT - 1, PITCH>(ve, va, cb);
     }
 }
 
 // The xi term diss_xi(alpha_u q) - diff_xi(Ehat) of closure columns I0 .. I0 + CNT - 1 at one end
 // of a line, for one component and tile row: e / a are the transposed Ehat / alpha_u q arrays at
-// the row, `lc` the local column of the block's first input; each sum scaled by idx as the
-// interior path scales it, into cb[i * kClosurePitch].
+// the row, `lc` the local column of the block's first input (the inputs carry the spacing
+// factor through the metrics), into cb[i * kClosurePitch].
 template <int OP, bool UPW, bool RIGHT, int XCH, int I0, int CNT>
-__device__ __forceinline__ void closure_xi(const float* __restrict__ e, const float* __restrict__ a, int lc, float idx,
+__device__ __forceinline__ void closure_xi(const float* __restrict__ e, const float* __restrict__ a, int lc,
                                            float* __restrict__ cb) {
     constexpr int N = OpShape<OP>::N;
     const int se = xslot<XCH>(lc) * kVecPitch, so = xslot<XCH>(lc + 1) * kVecPitch;
@@ -164,15 +162,15 @@ __device__ __forceinline__ void closure_xi(const float* __restrict__ e, const fl
         ve[k] = e[o];
         va[k] = UPW ? a[o] : 0.0f;
     }
-    closure_out<OP, UPW, RIGHT, I0, CNT>(ve, va, idx, cb);
+    closure_out<OP, UPW, RIGHT, I0, CNT>(ve, va, cb);
 }
 
 // The eta term diss_eta(alpha_v q) - diff_eta(Fhat) of closure rows I0 .. I0 + CNT - 1 at one
 // end of a column (BOTTOM = false: rows 0 .. M - 1, true: n - M .. n - 1), for one component and
 // tile column: f / a are the Fhat / alpha_v q arrays at the column, `lr` the local row of the
-// block's first input; each sum scaled by idx, into cb[i * kTileX].
+// block's first input, into cb[i * kTileX].
 template <int OP, bool UPW, bool BOTTOM, int I0, int CNT>
-__device__ __forceinline__ void closure_eta(const float* __restrict__ f, const float* __restrict__ a, int lr, float idx,
+__device__ __forceinline__ void closure_eta(const float* __restrict__ f, const float* __restrict__ a, int lr,
                                             float* __restrict__ cb) {
     constexpr int N = OpShape<OP>::N;
     float ve[N], va[N];
@@ -181,7 +179,7 @@ __device__ __forceinline__ void closure_eta(const float* __restrict__ f, const f
         ve[k] = f[(lr + k) * kTileX];
         va[k] = UPW ? a[(lr + k) * kTileX] : 0.0f;
     }
-    closure_out<OP, UPW, BOTTOM, I0, CNT, kTileX>(ve, va, idx, cb);
+    closure_out<OP, UPW, BOTTOM, I0, CNT, kTileX>(ve, va, cb);
 }
 
 // The two values of a thread's row u at columns c0, c0 + 1 from `p` (the element of (r0, c0)).
@@ -244,7 +242,6 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
         const InstanceDev& I = A.inst[B.instance];
         const float cbf = float(A.stage < 4 ? I.cb[A.stage] : 0.0);
         const float caf = float(A.stage < 3 ? I.ca[A.stage] : 0.0);
-        const float idxx = B.idx_xi_f, idxy = B.idx_eta_f;
 
         // ---------------- phase 1: pointwise quantities ----------------
         // One index space over all threads: eta-region points (local rows 0 .. eh - 1, 32 slots per
@@ -364,11 +361,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 const float* al = sE + (UPW ? 4 + comp : comp) * XA + r;
                 float* cb = cbuf + comp * MX * kClosurePitch + r;
                 if (right_cl) {
-                    if (half) closure_xi<OPX, UPW, true, XCH, MX / 2, MX / 2>(e, al, lc, idxx, cb);
-                    else closure_xi<OPX, UPW, true, XCH, 0, MX / 2>(e, al, lc, idxx, cb);
+                    if (half) closure_xi<OPX, UPW, true, XCH, MX / 2, MX / 2>(e, al, lc, cb);
+                    else closure_xi<OPX, UPW, true, XCH, 0, MX / 2>(e, al, lc, cb);
                 } else {
-                    if (half) closure_xi<OPX, UPW, false, XCH, MX / 2, MX / 2>(e, al, lc, idxx, cb);
-                    else closure_xi<OPX, UPW, false, XCH, 0, MX / 2>(e, al, lc, idxx, cb);
+                    if (half) closure_xi<OPX, UPW, false, XCH, MX / 2, MX / 2>(e, al, lc, cb);
+                    else closure_xi<OPX, UPW, false, XCH, 0, MX / 2>(e, al, lc, cb);
                 }
             }
         }
@@ -382,11 +379,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 const float* al = sF + (UPW ? 4 + comp : comp) * YA + col;
                 float* cb = cbuf_y + comp * MY * kTileX + col;
                 if (bot_cl) {
-                    if (half) closure_eta<OPY, UPW, true, MY / 2, MY / 2>(f, al, lr, idxy, cb);
-                    else closure_eta<OPY, UPW, true, 0, MY / 2>(f, al, lr, idxy, cb);
+                    if (half) closure_eta<OPY, UPW, true, MY / 2, MY / 2>(f, al, lr, cb);
+                    else closure_eta<OPY, UPW, true, 0, MY / 2>(f, al, lr, cb);
                 } else {
-                    if (half) closure_eta<OPY, UPW, false, MY / 2, MY / 2>(f, al, lr, idxy, cb);
-                    else closure_eta<OPY, UPW, false, 0, MY / 2>(f, al, lr, idxy, cb);
+                    if (half) closure_eta<OPY, UPW, false, MY / 2, MY / 2>(f, al, lr, cb);
+                    else closure_eta<OPY, UPW, false, 0, MY / 2>(f, al, lr, cb);
                 }
             }
         }
@@ -436,11 +433,11 @@ __global__ void __launch_bounds__(kStageThreads, 2) stage_kernel_vec(const Stage
                 // xi sums: ex[j] / dx[j] = column c0 + j over rows (r0, r0 + 1)
                 float2 ex[2], dx[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
                 float2 ey[2], ay[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
-                xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, idxx, ex);
-                if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, idxx, dx);
+                xi_pair<OPX, DIFF>(xwe + cc * XA, xwo + cc * XA, ex);
+                if constexpr (UPW) xi_pair<OPX, DISS>(xwe + (4 + cc) * XA, xwo + (4 + cc) * XA, dx);
                 // eta sums: ey[u] / ay[u] = row r0 + u over columns (c0, c0 + 1)
-                eta_pair<OPY, DIFF>(ewin + cc * YA, idxy, ey);
-                if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, idxy, ay);
+                eta_pair<OPY, DIFF>(ewin + cc * YA, ey);
+                if constexpr (UPW) eta_pair<OPY, DISS>(ewin + (4 + cc) * YA, ay);
                 if (xi_pre) {
 #pragma unroll
                     for (int j = 0; j < 2; ++j) {

@@ -295,15 +295,25 @@ cudaError_t narrow_f32(const double* in, float* out, int64_t n, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Plane 0 of each block's single-precision metrics holds 1 / J (rounded once from the f64
-// quotient), so the compensated stage kernels scale the flux divergence by a product.
+// The single-precision metrics of the compensated stage kernels: plane 0 holds 1 / J (rounded
+// once from the f64 quotient), so the flux divergence is scaled by a product; planes 1-2 (J dxi/dx,
+// J dxi/dy) are multiplied by the block's xi spacing factor idx_xi and planes 3-4 by idx_eta (in
+// f64, then rounded), so every stencil input of a direction carries its factor and the stencil
+// sums need no final scaling (the operators are linear and the dissipation coefficients are
+// homogeneous of degree one in the metrics).
 __global__ void jacobian_inverse_kernel(const BlockDev* __restrict__ blocks, const double* __restrict__ met64,
                                         float* __restrict__ met32) {
     const BlockDev& B = blocks[blockIdx.y];
-    const int64_t n = (int64_t)B.nx * B.ny;
+    const int64_t n = (int64_t)B.nx * B.ny, np = B.npad;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double j = met64[B.m_off + i];
-        met32[B.m_off + i] = j != 0.0 ? float(1.0 / j) : 0.0f;
+        const double* m = met64 + B.m_off + i;
+        float* o = met32 + B.m_off + i;
+        const double j = m[0];
+        o[0] = j != 0.0 ? float(1.0 / j) : 0.0f;
+        o[np] = float(m[np] * B.idx_xi);
+        o[2 * np] = float(m[2 * np] * B.idx_xi);
+        o[3 * np] = float(m[3 * np] * B.idx_eta);
+        o[4 * np] = float(m[4 * np] * B.idx_eta);
     }
 }
 
