@@ -98,3 +98,23 @@ def test_micro_tile_against_f64_oracle(orc):
     o.advance(cfg.steps, cfg.dt)
     assert rel_l2(g.state(0), o.state(0)) <= 1e-5
     g.close()
+
+
+@pytest.mark.parametrize("op_name,sizes", [
+    ("upwind9", [(16, 17), (20, 33), (39, 40), (41, 64), (65, 71)]),
+    ("upwind4", [(8, 9), (12, 35), (36, 37), (64, 33)]),
+])
+def test_closure_tile_split(op_name, sizes):
+    """Lines whose closure rows would straddle a tile boundary or share a tile with the other
+    end's closure (lengths 2 M .. 2 tiles, multiples of 32 and 32 k + 1 .. 32 k + M - 1): the tile
+    lists move the boundary so one tile holds each end, and both kernels still agree."""
+    from summationbyparts_b200 import operators, workloads
+    from summationbyparts_b200.system import BC_VORTEX, BlockSpec
+    op = operators.BY_NAME[op_name]()
+    blocks = []
+    for k, (nx, ny) in enumerate(sizes):
+        x, y = workloads.warped(-5.0, 5.0, nx, -5.0, 5.0, ny)
+        blocks.append(BlockSpec(x, y, op, [(BC_VORTEX, 0)] * 4, k))
+    vortex = workloads.STANDARD_VORTEX
+    a, b = _both(blocks, 6, ninst=len(sizes), per_instance=[(vortex, 0.002)] * len(sizes))
+    assert rel_l2(b, a) <= BAR
