@@ -2,8 +2,9 @@
 // ensembles of independent solves (instances), behind the C ABI.
 //
 // Per RK4 step the device runs, for each of the 4 stages, one persistent fused stage kernel per
-// operator pair present (all tiles of all active blocks of that pair in one launch), then one
-// tiny kernel that advances the instance times.  The whole step is captured once as a CUDA
+// operator pair present (all tiles of all active blocks of that pair in one launch) and its edge
+// kernel (uncoupled operator groups on their own streams, joined once per step), then one tiny
+// kernel that advances the instance times.  The whole step is captured once as a CUDA
 // graph and replayed; the graph is re-captured only when the tile schedule or the set of
 // active instances changes.
 #include <cuda_runtime.h>
@@ -537,6 +538,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
         }
     }
     std::vector<std::vector<int4>> tiles(groups.size()), edges(groups.size());
+    std::vector<int> group_of(s->nblocks, -1);
     for (int b = 0; b < s->nblocks; ++b) {
         const BlockDev& B = s->hb[b];
         if (!active[B.instance]) continue;
@@ -547,6 +549,7 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
         size_t gi = 0;
         for (; gi < groups.size(); ++gi)
             if (groups[gi].opx == B.op_xi && groups[gi].opy == B.op_eta && groups[gi].upw == upw) break;
+        group_of[b] = (int)gi;
         Group& g = groups[gi];
         const int TY = g.ty;
         const std::vector<int> ys = tile_starts(B.ny, TY, oy.M), xs = tile_starts(B.nx, TX, ox.M);
@@ -628,10 +631,33 @@ sbp_status build_step_graph(sbp_system* s, const std::vector<int>& active, const
         s->side.push_back(st);
         s->ev.push_back(e);
     }
+    // Groups are independent when no block reads an edge of a block of another group (Grid and
+    // Interpolate neighbours; MultiGrid sides are taken as coupling).  Independent groups run their
+    // four stages on their own streams and join once per step, so one group's edge kernel can run
+    // beside another group's stage kernel; coupled groups join after every stage.
+    bool coupled = false;
+    for (int b = 0; b < s->nblocks && !coupled; ++b) {
+        if (group_of[b] < 0) continue;
+        const BlockDev& B = s->hb[b];
+        for (int d = 0; d < 4; ++d) {
+            const int k = B.bc_kind[d];
+            if (k == BC_MULTIGRID || ((k == BC_GRID || k == BC_INTERPOLATE) && group_of[B.bc_nb[d]] != group_of[b]))
+                coupled = true;
+        }
+    }
     // Capture one RK4 step.
     SBP_TRY_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     sbp_status rc = SBP_OK;
-    for (int stage = 0; stage < 4 && rc == SBP_OK; ++stage) {
+    if (groups.size() > 1 && !coupled) {
+        cudaEventRecord(s->ev_fork, s->stream);
+        for (size_t gi = 0; gi < groups.size() && rc == SBP_OK; ++gi) {
+            cudaStreamWaitEvent(s->side[gi], s->ev_fork, 0);
+            for (int stage = 0; stage < 4 && rc == SBP_OK; ++stage) rc = launch_group(s, stage, groups[gi], s->side[gi]);
+            cudaEventRecord(s->ev[gi], s->side[gi]);
+        }
+        for (size_t gi = 0; gi < groups.size(); ++gi) cudaStreamWaitEvent(s->stream, s->ev[gi], 0);
+    }
+    for (int stage = 0; stage < 4 && rc == SBP_OK && (groups.size() == 1 || coupled); ++stage) {
         if (groups.size() == 1) {
             rc = launch_group(s, stage, groups[0], s->stream);
         } else {
