@@ -18,7 +18,8 @@ Fallback: the indicator of a case is a residual of the corrected output, the rel
 of the network's correction, |corrected - coarse| / |coarse|.  The network learned corrections
 of the sizes the training cases needed; a case that it corrects by more than ``FALLBACK_FACTOR``
 times the largest correction it applies to any training case is outside what it was trained on,
-and is solved on the fine grid instead (the fine FP64 solve is both the judge and the fallback).
+and is solved on the fine grid instead (the fine FP64 solve is both the error reference and the
+fallback).
 The indicator costs one norm per case, no second solve.
 
     python -m summationbyparts_b200.learned --pairs 4096 --heldout 512 --epochs 40 --json out.json
@@ -278,7 +279,7 @@ def run(pairs: int, heldout: int, epochs: int, fine: int = FINE, lr: float = 2e-
     t_train = time.perf_counter() - t1
     threshold = fallback_factor * float(indicator(net.apply(train_c), train_c).max())
 
-    # held-out cases: the fine solve judges (and is the fallback); the coarse path is timed
+    # held-out cases: the fine solve is the error reference (and the fallback); the coarse path is timed
     cases = draws(heldout, pairs)
     coarse, t_coarse = solve(cases, COARSE, UPWIND4, "f32c", device)
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))

@@ -136,7 +136,7 @@ def test_training_gains_over_coarse():
 
 def test_fallback_replaces_flagged_cases_by_the_fine_solve():
     """The fallback path: with the threshold scaled far down every held-out case is flagged, so
-    the answer of each is its restricted fine f64 solve (no error against the judge) and the
+    the answer of each is its restricted fine f64 solve (no error against the fine solve) and the
     fallback solves enter the time to solution."""
     from summationbyparts_b200 import learned
     rep = learned.run(pairs=16, heldout=8, epochs=5, fine=128, lr=3e-3, max_batch=16, fallback_factor=1e-9)
